@@ -1,0 +1,394 @@
+"""Throughput benchmark: cell-updates/s of the explicit FV loop on one B200.
+
+Workload (default): the 3D ramp channel (x in [0,3], y in [0,1], z in [0,1],
+12 deg ramp from x = 0.5 up to y = 0.2) meshed as 200x100x50 hexes split into
+6 tetrahedra each = 6,000,000 tets; Mach 3, p = 101325 Pa, T = 300 K;
+HLLC flux, cell-limited MUSCL with the Venkatakrishnan limiter (K = 5),
+Green-Gauss gradients, RK4 (the reference's standard coefficients),
+LocalAccTime1 evaluated from stage-start values, CFL 0.5; FP32 state and
+fluxes, FP64 geometry / RK state / residual norms; cells on a Hilbert curve.
+One step = one iteration (4 RK stages) over all cells. Synthetic mesh and
+freestream start: no dataset is involved.
+
+  value : cell-updates/s with the state resident in HBM (K iterations in one
+          psst_explicit_solve call, CUDA events on the solver's stream)
+  e2e   : same metric through the C ABI with host buffers: the initial state
+          copied from pinned host memory, K per-iteration psst_explicit_solve
+          calls each returning its residual columns to the host, the final
+          state copied back -- all inside the timed region
+  roofline: the dominant kernel's algorithmic bytes per launch over its mean
+          launch time (psst_solver_profile), against the measured HBM peak
+  cpu_baseline: the reference compiled from its own sources (oracle/_ref),
+          one process per host core, on a reduced mesh of the same workload
+
+--impl reference runs the reference's CPU implementation of the path on the
+host cores instead and prints the same metric.
+Multi-GPU: the path runs as independent replicas (one case per GPU, no
+collective); value = all ranks' cell-updates / max rank time.
+"""
+import argparse
+import glob
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nx, ny, nz, mach, angle)
+    "wedge3d_6M_tets": (200, 100, 50, 3.0, 12.0),
+    "wedge3d_750k_tets": (100, 50, 25, 3.0, 12.0),  # small case for ncu captures
+}
+SCHEME = dict(flux=3, order=2, limiter=5, grad=1, lc=1, rk_level=4, cfl=0.5)
+CPU_SAMPLE = (40, 20, 4)  # reduced mesh of the same workload for the CPU reference: 19,200 tets
+CPU_SAMPLE_SCHEME = dict(SCHEME, limiter=3)  # the reference has no Venkatakrishnan limiter: VanLeer/DM
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_case(workload, directory):
+    from supersonicflowsolver_b200 import meshgen
+    from supersonicflowsolver_b200.psst import Grid
+
+    nx, ny, nz, mach, angle = WORKLOADS[workload]
+    mesh = meshgen.wedge3d(nx, ny, nz, angle, tets=True)
+    zones = [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
+    meshgen.write_case(directory, "bench", dim=3, zones=zones, mach=mach, max_iter=1, **SCHEME)
+    grid = Grid.from_mesh(mesh)
+    del mesh
+    sc, prim = grid.read_case(directory, "bench")
+    sc.precision = 32
+    sc.lc1_mode = 1
+    sc.renumber = 1
+    return grid, sc, prim
+
+
+def traffic_model(grid, nnz, kind):
+    """Algorithmic (compulsory) DRAM bytes per launch of each kernel for the FP32
+    3D MUSCL/Venkatakrishnan configuration: every array touched once, neighbour
+    data counted once per cell (perfect on-chip reuse). s = 4 B state word,
+    g = 8 B geometry word, i = 4 B index."""
+    nint, ngh, nf = grid.ninterior, grid.nghost, grid.nface
+    K = nnz / nint
+    if kind == "face_flux":
+        # per face: c0,c1 (2i) + S (g) + n (3g) + x_f (3g) read, flux*area (5s) written;
+        # per interior cell: p,T,rho,u (6s) + grads (15s) + limiter (5s) + centroid (3g); ghosts 6s
+        return nf * (8 + 8 + 24 + 24 + 20) + nint * (24 + 60 + 20 + 24) + ngh * 24
+    if kind == "cell_update":
+        # per cell: CSR ptr (i) + K entries (i) + own-order perm (8) + V (g) + own T,u (4s)
+        # + w, prev_w (FP64, 2x5x8, a third on stage 0 amortised) + new p,T,rho,u (6s) + dt (g);
+        # per face: flux*area (5s) + S, n for the time step (4g)
+        return nint * (4 + 4 * K + 8 + 8 + 16 + 80 + 10 + 24 + 8) + nf * (20 + 32)
+    if kind == "gradient":
+        # per cell: CSR (i + K i) + perm + V + eps^2 + own p,T,u (5s) + centroid (3g)
+        # + gradients (15s) + limiter (5s) written; per face: beta, S, n, x_f (8g); ghosts 5s
+        return nint * (4 + 4 * K + 8 + 8 + 8 + 20 + 24 + 60 + 20) + nf * 64 + ngh * 20
+    if kind == "ghost_update":
+        return ngh * (12 + 20 + 20 + 24 + 24)
+    return 0
+
+
+def read_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel>_<workload>.txt, line 'dram_bytes_per_launch_full_size: N')."""
+    path = os.path.join(ROOT, "profiles", "%s_%s.txt" % (kernel, workload))
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_full_size:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU side ---
+def reference_binary():
+    ref = os.path.join(ROOT, "oracle", "_ref", "psst_ref")
+    if os.path.exists(ref):
+        return ref, "reference"
+    port = os.path.join(ROOT, "oracle", "_build", "psst_oracle")
+    if not os.path.exists(port):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "port"], capture_output=True)
+    return port, "port"
+
+
+def cpu_run(n_iter, procs):
+    """Runs the reference (or the oracle port where the reference was not built)
+    on the reduced mesh, `procs` independent processes, n_iter iterations each.
+    Returns per-process per-iteration loop times (s) from the residual file's
+    time column (mesh reading and setup excluded, as the reference prints)."""
+    from supersonicflowsolver_b200 import meshgen
+
+    exe, kind = reference_binary()
+    nx, ny, nz = CPU_SAMPLE
+    mach, angle = WORKLOADS["wedge3d_6M_tets"][3:5]
+    base = tempfile.mkdtemp(prefix="psst_cpu_")
+    mesh = meshgen.wedge3d(nx, ny, nz, angle, tets=True)
+    zones = [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
+    meshgen.write_fluent(mesh, os.path.join(base, "m.msh"))
+    runs = []
+    for p in range(procs):
+        d = os.path.join(base, "p%d" % p)
+        os.makedirs(d)
+        os.link(os.path.join(base, "m.msh"), os.path.join(d, "m.msh"))
+        meshgen.write_case(d, "c", dim=3, zones=zones, mach=mach, max_iter=n_iter, save_step=10 ** 6,
+                           **CPU_SAMPLE_SCHEME)
+        open(os.path.join(d, "problem_manager"), "w").write("m.msh\nc")
+        runs.append(subprocess.Popen([exe], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+    for r in runs:
+        r.wait()
+    times = []
+    for p in range(procs):
+        f = os.path.join(base, "p%d" % p, "c_residual.dat")
+        rows = [l.split() for l in open(f) if l.strip()] if os.path.exists(f) else []
+        if len(rows) == n_iter:
+            times.append([float(r[1]) for r in rows])
+    shutil.rmtree(base, ignore_errors=True)
+    return times, kind, mesh.ncells, exe
+
+
+def cpu_baseline(warm, steps, procs):
+    times, kind, ncells, exe = cpu_run(warm + steps, procs)
+    if not times:
+        return None
+    # the time column is cumulative ms-resolution wall time since the loop began
+    span = [t[warm + steps - 1] - (t[warm - 1] if warm > 0 else 0.0) for t in times]
+    rate = sum(ncells * steps / s for s in span if s > 0)
+    return {"value": rate, "unit": "cell-updates/s", "cores": len(times), "kind": kind,
+            "sample": "%d tets (%dx%dx%d hexes x6, same ramp/Mach/scheme, DM+VanLeer limiter), "
+                      "%d timed + %d warm-up iterations per process, %d processes" %
+                      (ncells, *CPU_SAMPLE, steps, warm, len(times)),
+            "binary": os.path.relpath(exe, ROOT)}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    procs = max(1, os.cpu_count() or 1)
+    times, kind, ncells, exe = cpu_run(args.warmup + args.steps, procs)
+    if not times:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference binary produced no residual file"}))
+        return
+    span = [t[-1] - t[args.warmup - 1] for t in times]
+    value = sum(ncells * args.steps / s for s in span if s > 0)
+    ms = 1000.0 * max(span) / args.steps
+    print(json.dumps({
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "wedge3d_6M_tets (CPU sample %d tets)" % ncells, "scheme": "HLLC + DM/VanLeer, GG, RK4, "
+                   "LocalAccTime1, CFL 0.5, Mach 3, 12 deg", "parallelism": "%d independent processes" % len(times)},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": len(times), "kind": kind,
+                         "sample": "%d tets per process, %d timed + %d warm-up iterations" %
+                                   (ncells, args.steps, args.warmup)},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------- GPU side ---
+def run_gpu(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local
+    torch.cuda.set_device(dev)
+    from supersonicflowsolver_b200.psst import Solver
+
+    tmp = tempfile.mkdtemp(prefix="psst_bench_")
+    grid, sc, prim = build_case(args.workload, tmp)
+    solver = Solver(grid, sc, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_state(prim)
+    nint = grid.ninterior
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    solver.explicit_solve(args.warmup)
+    barrier()
+    # device-resident timed region; inputs (~2.6 GB of mesh + state) exceed the 126 MB L2
+    with ClockSampler(dev) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(stream)
+        linf, _ = solver.explicit_solve(args.steps)
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        launches, lib_ms = solver.last_stats()
+        # end-to-end through the C ABI with host buffers
+        host_prim = torch.from_numpy(prim).pin_memory()
+        barrier()
+        t0 = time.perf_counter()
+        solver.set_state(host_prim.numpy())
+        for _ in range(args.steps):
+            solver.explicit_solve(1)
+        out = solver.get_state()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    clocks = clk.summary()
+    ms_max = ms
+    e2e_max = e2e_s
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms, e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max, e2e_max = float(t[0]), float(t[1])
+    value = ws * nint * args.steps / (ms_max / 1000.0)
+    e2e_value = ws * nint * args.steps / e2e_max
+    # per-kernel timing for the roofline (CUDA events around each launch)
+    prof = solver.profile(2)
+    nnz = 2 * grid.nface - grid.nghost  # CSR entries: interior faces twice, boundary faces once
+    kernel, (kms, kcnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    algo = traffic_model(grid, nnz, kernel)
+    peak, peak_kind = peaks()
+    achieved = algo / (kms / kcnt / 1000.0) / 1e9
+    traffic = read_traffic(kernel, args.workload)
+    finite = bool(np.all(np.isfinite(linf))) and bool(np.all(np.isfinite(out)))
+    if rank == 0:
+        nv = grid.dim + 2
+        state_bytes = (2 + grid.dim) * grid.nvol * 8
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "cells": nint, "faces": grid.nface,
+                       "scheme": "HLLC + MUSCL/Venkatakrishnan(K=5), Green-Gauss, RK4 std, LocalAccTime1 "
+                                 "(stage-start values), CFL 0.5, Mach 3, 12 deg ramp",
+                       "precision": "FP32 state/flux; FP64 geometry, RK state, residual norms",
+                       "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "l2_flush": "not needed: >2.5 GB of mesh + state per step, L2 is 126 MB"},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": (state_bytes / args.steps) + 2 * nv * 8 + 16,
+                    "note": "set_state from pinned host memory + K psst_explicit_solve(1) calls each returning "
+                            "residual columns + get_state, all timed"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_launch": algo, "launch_ms": kms / kcnt,
+                         "traffic": traffic},
+            "kernel_ms_per_iteration": {k: v[0] / 2 for k, v in prof.items()},
+            "library_device_ms": lib_ms,
+            "finite": finite,
+        }
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(1, 2, max(1, os.cpu_count() or 1))
+            line["cpu_baseline"] = cb
+        print(json.dumps(line))
+    solver.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="wedge3d_6M_tets", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

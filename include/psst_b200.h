@@ -1,0 +1,236 @@
+/* psst_b200.h — C ABI of libpsst_b200.so, the B200 (sm_100a) implementation of
+ * PSST's explicit finite-volume residual/update loop.
+ *
+ * The reference exposes this path as C++ strategy interfaces selected by the
+ * factory in psstGridFV::solver_parameters (psstFiniteVolumeGrid.cpp:36-194)
+ * and driven by psstGridFV::explicit_solve (psstFiniteVolumeGrid.cpp:248-401).
+ * Per-face virtual calls cannot cross a host/device boundary, so this ABI cuts
+ * at stage and iteration granularity. Every entry point below names the
+ * reference interface it replaces.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, status codes. No exceptions cross the
+ *    ABI; a failing call returns a non-zero psst_status and psst_last_error()
+ *    returns its message (thread-local). Messages reuse the reference's texts
+ *    where the reference reports the same condition.
+ *  - Buffers passed in are caller-owned and copied; buffers passed out are
+ *    caller-allocated with the stated size.
+ *  - Volumes are numbered in the reference's storage order: all volume zones in
+ *    ascending zone id (std::map order), interior cells and ghost cells alike,
+ *    each zone in its own index order (psstFiniteVolumeGrid.h:23). Faces are
+ *    numbered in the reference's face-loop order: face zones in ascending id,
+ *    each in file order (psstFiniteVolumeGrid.h:21).
+ *  - Primitive state arrays are SoA: p[nvol], T[nvol], u[dim][nvol] packed as
+ *    prim[(2 + dim) * nvol] = {p..., T..., u0..., u1..., (u2...)}.
+ *  - A psst_solver owns its device memory and one CUDA stream; it is not
+ *    thread-safe. Calls on one solver are stream-ordered.
+ */
+#ifndef PSST_B200_H
+#define PSST_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSST_B200_ABI_VERSION 1
+
+typedef enum psst_status {
+    PSST_OK = 0,
+    PSST_ERR_ARG = 1,         /* invalid argument (reference: std::invalid_argument) */
+    PSST_ERR_IO = 2,          /* file missing/unreadable */
+    PSST_ERR_FORMAT = 3,      /* malformed mesh or setup file */
+    PSST_ERR_CUDA = 4,        /* CUDA runtime error, or no usable device */
+    PSST_ERR_NONFINITE = 5,   /* non-finite residual or state detected on the device */
+    PSST_ERR_FLUX = 6,        /* HLL/HLLC wave speeds not ordered (ConvectiveFlow.cpp:283-286, 582-585) */
+    PSST_ERR_TIMEOUT = 7,     /* a bounded device-side wait ran out */
+    PSST_ERR_UNSUPPORTED = 8, /* option the reference does not support either */
+    PSST_ERR_STATE = 9        /* call order violated (e.g. no state set) */
+} psst_status;
+
+typedef struct psst_grid psst_grid;     /* host mesh + geometry, reference storage order */
+typedef struct psst_solver psst_solver; /* device state for one case */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *psst_last_error(void);
+int psst_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Mesh                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Reads a Fluent ASCII mesh (.msh/.cas; LF or CRLF) and builds the finite-volume
+ * grid: ghost cell per boundary face, face/volume wiring, FP64 geometry.
+ * Replaces psstAnsysDirector::construct_grid (psstAnsysGridReader.cpp:1308-1317)
+ * + psstAnsysInputGrid::create_finite_volume_grid (psstAnsysGridReader.cpp:688-907)
+ * + psstFace::initialize / psstVolume::initialize
+ *   (psstFiniteVolumeGridTools.cpp:397-505, 709-827). */
+psst_status psst_grid_read_fluent(const char *path, psst_grid **out);
+
+/* Same grid from in-memory Fluent-style arrays (for callers that already hold
+ * the mesh, e.g. a reference-side shim or a mesh generator). Faces are given in
+ * file order grouped in zones; cells are given per cell zone.
+ *  face_nodes: 0-based vertex ids, face_ptr[nface+1] offsets into it;
+ *  face_c0/face_c1: 0-based cell ids, -1 = none (Fluent's 0);
+ *  zones: for each zone in file order, id, Fluent bc type, first and last
+ *  1-based index (cells or faces, per bc type) and a name. */
+typedef struct psst_zone_desc {
+    int64_t id, bc_type, first, last;
+    const char *name;
+} psst_zone_desc;
+
+typedef struct psst_fluent_desc {
+    int32_t dim;
+    int64_t nvert;
+    const double *verts; /* nvert * dim */
+    int64_t nface;
+    const int64_t *face_ptr;   /* nface + 1 */
+    const int64_t *face_nodes; /* face_ptr[nface] */
+    const int64_t *face_c0, *face_c1;
+    int64_t ncell;
+    int32_t nzone;
+    const psst_zone_desc *zones;
+} psst_fluent_desc;
+
+psst_status psst_grid_from_fluent(const psst_fluent_desc *desc, psst_grid **out);
+
+typedef struct psst_grid_info {
+    int32_t dim;
+    int64_t nvol;      /* all volumes (interior + ghost) */
+    int64_t ninterior; /* volumes of interior cell zones (bc 1) */
+    int64_t nghost;    /* ghost volumes (one per boundary face) */
+    int64_t nface;     /* all faces of all face zones */
+    int32_t max_faces_per_cell;
+    double min_vol; /* psstGridFV::min_vol (psstAnsysGridReader.cpp:886-905) */
+} psst_grid_info;
+
+psst_status psst_grid_get_info(const psst_grid *g, psst_grid_info *out);
+
+/* Copies a named array in reference order. Doubles: "vol_V", "vol_x"[nvol*dim],
+ * "face_S", "face_n"[nface*dim], "face_x"[nface*dim], "face_beta". Int64:
+ * "face_c0", "face_c1" (volume index, -1 none), "vol_zone", "vol_boundary",
+ * "face_zone". count = element count of the out buffer. */
+psst_status psst_grid_get_array(const psst_grid *g, const char *name, void *out, int64_t count);
+
+void psst_grid_free(psst_grid *g);
+
+/* ------------------------------------------------------------------------ */
+/* Case setup                                                                */
+/* ------------------------------------------------------------------------ */
+
+enum { PSST_FLUX_AUSM = 1, PSST_FLUX_HLL = 2, PSST_FLUX_HLLC = 3 };
+enum { PSST_GRAD_GREEN_GAUSS = 1, PSST_GRAD_LEAST_SQUARES = 2 };
+/* 1..3 are the reference's psstScalarLimiters (DM reconstruction); 4 and 5 are
+ * cell-based MUSCL limiters the reference does not have. */
+enum {
+    PSST_LIMITER_VANALBADA = 1,
+    PSST_LIMITER_MINMOD = 2,
+    PSST_LIMITER_VANLEER = 3,
+    PSST_LIMITER_BARTH_JESPERSEN = 4,
+    PSST_LIMITER_VENKATAKRISHNAN = 5
+};
+/* Local time step: 0 psstUniformTime, 1 psstLocalAccTime1, 2 psstLocalAccTime2 */
+enum { PSST_TIME_UNIFORM = 0, PSST_TIME_LOCAL1 = 1, PSST_TIME_LOCAL2 = 2 };
+/* lc1_mode for PSST_TIME_LOCAL1: the reference evaluates it inside the update
+ * loop, so each cell sees neighbours already updated in the same stage
+ * (psstFiniteVolumeGrid.cpp:323). SEQUENTIAL reproduces that exactly with a
+ * level schedule; JACOBI uses stage-start values for every cell. */
+enum { PSST_LC1_SEQUENTIAL = 0, PSST_LC1_JACOBI = 1 };
+
+typedef struct psst_scheme {
+    int32_t flux, order, grad, limiter;
+    int32_t lc, lc1_mode;
+    int32_t rk_level;
+    double rk[16];
+    double cfl;
+    double rm, cp, cv, gamma; /* gas constants as psstGridFV derives them */
+    double ref_vel;           /* psstUniformTime reference speed */
+    double venkat_k;          /* Venkatakrishnan K (limiter 5) */
+    int32_t precision;        /* 64: FP64 parity path; 32: FP32 production path */
+    int32_t renumber;         /* 1: reorder cells along a Hilbert curve on the device */
+    int64_t iter, max_iter, iter_step; /* reference counters (.inp lines 4-5, .sav) */
+} psst_scheme;
+
+/* Reads <dir>/<name>.inp/.prop/.par (or .sav)/.bvp/.btq exactly as
+ * psstGridFV::solver_parameters does (psstFiniteVolumeGrid.cpp:36-194,
+ * 403-557, 559-604, 641-717). Boundary conditions are attached to the grid;
+ * the scheme is returned; prim (may be NULL) receives the initial primitive
+ * state of every volume including ghosts ((2+dim)*nvol doubles). */
+psst_status psst_case_read(psst_grid *g, const char *dir, const char *name, psst_scheme *scheme,
+                           double *prim);
+
+/* Boundary conditions set directly (same ids as .bvp/.btq): dynamic 23, 26, 15,
+ * 25; thermal 27, 25, 11, 18. u has dim entries (23), p (23, 25), T (27, 11). */
+psst_status psst_grid_set_boundary(psst_grid *g, const char *zone_name, int dyn_id, const double *u,
+                                   double p, int therm_id, double T);
+
+/* ------------------------------------------------------------------------ */
+/* Solver                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* Uploads grid and scheme to `device`. Replaces the strategy construction and
+ * initialize() calls in solver_parameters (psstFiniteVolumeGrid.cpp:50-192). */
+psst_status psst_solver_create(const psst_grid *g, const psst_scheme *scheme, int device,
+                               psst_solver **out);
+
+/* Sets the primitive state of all volumes and forms w as the explicit_solve
+ * prologue does (psstFiniteVolumeGrid.cpp:279-300). */
+psst_status psst_solver_set_state(psst_solver *s, const double *prim);
+
+/* Reads back primitives ((2+dim)*nvol) and, if w != NULL, the conservative
+ * state w[(dim+2)*nvol] (rho*u.., rho, rho*E; zero for ghosts). */
+psst_status psst_solver_get_state(psst_solver *s, double *prim, double *w);
+
+/* psstInterfaceGradientCalc::calculate (psstGradCalculation.h:20;
+ * psstGreenGauss .cpp:80-177, psstLeastSquare .cpp:268-368). For limiters 4/5
+ * this also evaluates the cell limiter. */
+psst_status psst_gradient_calculate(psst_solver *s);
+
+/* psstInterfaceConvectiveFlow::calculate (psstConvectiveFlow.h:22): face fluxes
+ * with the selected reconstruction/limiter, accumulated into per-cell residuals
+ * in the reference's face-loop order. */
+psst_status psst_convective_calculate(psst_solver *s);
+
+/* Stage k of psstRungeKutta (psstFiniteVolumeGrid.cpp:312-366): local time
+ * step (psstInterfaceLocalTime::calculate_at), w = prev_w - dt*a_k*res/V,
+ * primitives, then ghost boundary conditions
+ * (psstInterfaceBoundaryCondition::calculate_at). res_linf (may be NULL)
+ * receives max|residual| per component over interior cells. */
+psst_status psst_stage_update(psst_solver *s, int k, double *res_linf);
+
+/* n_iter iterations of the explicit_solve loop body (psstFiniteVolumeGrid.cpp:
+ * 305-367), launched back to back on the solver's stream. res_linf/res_l2 (may
+ * be NULL) receive n_iter*(dim+2) values: the reference's residual columns
+ * (max over stages and cells of |residual|) and RMS residuals. */
+psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *res_linf, double *res_l2);
+
+/* Debug/parity reads of device arrays, reference volume order:
+ * "residual"[(dim+2)*nvol], "dt"[nvol], "grad_u"[nvol*dim*dim],
+ * "grad_p"[nvol*dim], "grad_T"[nvol*dim], "limiter"[nvol*(dim+2)]. */
+psst_status psst_solver_get_array(psst_solver *s, const char *name, double *out, int64_t count);
+
+/* Runs the solver's work on the given CUDA stream (cudaStream_t passed as a
+ * pointer) instead of its own; NULL restores its own stream. */
+psst_status psst_solver_set_stream(psst_solver *s, void *stream);
+
+/* Kernel launches issued by the last psst_explicit_solve call, and the
+ * device-side duration (ms) of that call measured with CUDA events. */
+psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, double *device_ms);
+
+/* Runs n_iter iterations like psst_explicit_solve, with a CUDA event pair
+ * around every kernel launch, and returns per kernel kind the summed device
+ * time (ms) and the launch count. Kinds: 0 gradient (+cell limiter), 1 face
+ * flux, 2 cell update, 3 ghost update, 4 residual-norm finish. */
+#define PSST_KERNEL_KINDS 5
+psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind);
+
+/* Reference counter psstGridFV::iter_ after the calls so far. */
+int64_t psst_solver_iter(const psst_solver *s);
+
+void psst_solver_destroy(psst_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

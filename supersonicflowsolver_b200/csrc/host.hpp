@@ -1,0 +1,80 @@
+// Internal host-side data model of libpsst_b200 (not part of the C ABI).
+//
+// psst_grid holds the finite-volume grid in the reference's storage order
+// (volume zones and face zones in ascending zone id, psstFiniteVolumeGrid.h:21-23)
+// as flat arrays, plus everything the device layout is derived from.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "psst_b200.h"
+
+namespace psst {
+
+// Thrown inside the library only; every C entry point converts it to a status.
+struct Error {
+    psst_status status;
+    std::string msg;
+};
+[[noreturn]] void raise(psst_status st, const std::string &msg);
+void set_last_error(const std::string &msg);
+
+struct Zone {  // psstSimpleStorage (psstAnsysGridReader.h)
+    int64_t id = 0, first = 0, last = 0, bc = 0, size = 0;
+    std::string name;
+};
+
+// What a Fluent file says (psstAnsysInputGrid).
+struct RawMesh {
+    int dim = 0;
+    std::vector<double> verts;            // nvert * dim
+    std::vector<int64_t> face_ptr{0};     // per file face, into face_nodes
+    std::vector<int64_t> face_nodes;      // 1-based vertex ids
+    std::vector<int64_t> face_c0, face_c1;  // 1-based file cell ids, 0 = none
+    std::vector<int64_t> cell_zone;       // per file cell
+    std::vector<Zone> zones;              // file order (first appearance)
+    int64_t zone_slot(int64_t id);        // find or append
+};
+
+RawMesh read_fluent(const std::string &path);
+
+struct VZone {
+    int64_t id, bc, first, count;  // volumes [first, first+count)
+    std::string name;
+    int dyn = 0, therm = 0;        // .bvp / .btq ids
+    double u[3] = {0, 0, 0}, p = 0, T = 0;
+};
+struct FZone {
+    int64_t id, bc, first, count;
+    std::string name;
+};
+
+struct psst_grid_impl;
+}  // namespace psst
+
+struct psst_grid {
+    int dim = 0;
+    std::vector<psst::VZone> vz;  // ascending id
+    std::vector<psst::FZone> fz;  // ascending id
+    int64_t nvol = 0, nface = 0, ninterior = 0, nghost = 0;
+    std::vector<uint8_t> vol_boundary;   // ghost flag
+    std::vector<int32_t> vol_vz;         // volume -> vz slot
+    std::vector<int64_t> vf_ptr, vf_idx; // per volume face list, reference wiring order
+    std::vector<double> V, xc;           // nvol, nvol*dim
+    std::vector<int64_t> f_c0, f_c1;     // nface, volume index or -1
+    std::vector<int32_t> f_fz;           // face -> fz slot
+    std::vector<double> S, n, xf, beta;  // nface, nface*dim, nface*dim, nface
+    std::vector<double> lsq_r;           // 3 per zone-local interior index (2D least squares)
+    double min_vol = -1.0;
+    int max_faces = 0;
+    // initial state holder filled by psst_case_read (SoA p,T,u..)
+    std::vector<double> prim0;
+    double ref_vel = 0.0;
+};
+
+namespace psst {
+psst_grid *build_grid(const RawMesh &m);
+void compute_lsq(psst_grid &g);
+}  // namespace psst

@@ -1,0 +1,33 @@
+// Kernel launchers, one set per state precision (explicitly instantiated in
+// kernels_f64.cu and kernels_f32.cu). Host code (solver.cpp) calls only these.
+#pragma once
+#include <cuda_runtime_api.h>
+
+#include "devgrid.hpp"
+
+namespace psst {
+
+constexpr int kBlock = 256;
+inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+template <typename R>
+struct Ops {
+    static void prologue(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
+                         cudaStream_t s);
+    // grad: 1 Green-Gauss, 2 least squares; celllim: 0, 4 (Barth-Jespersen), 5 (Venkatakrishnan)
+    static void gradient(int dim, int grad, int celllim, const DevGrid &g, const DevState<R> &st,
+                         const DevWork<R> &wk, cudaStream_t s);
+    // rec: 0 first order, 1 DM with limiter lim (1..3), 2 cell-limited MUSCL
+    static void face_flux(int dim, int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st,
+                          const DevWork<R> &wk, const Gas &gas, cudaStream_t s);
+    static void residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStream_t s);
+    // lc: 0, 1, 2; seq: sequential LocalAccTime1 (single block over levels)
+    static void cell_update(int dim, int lc, bool seq, bool gather, const DevGrid &g, const DevState<R> &cur,
+                            const DevState<R> &nxt, const DevWork<R> &wk, const Gas &gas, double cfl,
+                            double dt_uniform, double alpha, int first_stage, int it_slot, cudaStream_t s);
+    static void ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
+                             const Gas &gas, cudaStream_t s);
+    static void l2_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s);
+};
+
+}  // namespace psst

@@ -1,0 +1,152 @@
+// Launcher bodies for Ops<R>: template dispatch from runtime scheme options to
+// kernel instantiations. Included by kernels_f64.cu / kernels_f32.cu only.
+#pragma once
+#include "kernels.cuh"
+#include "ops.hpp"
+
+namespace psst {
+
+template <typename R>
+void Ops<R>::prologue(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
+                      cudaStream_t s) {
+    if (g.nall == 0) return;
+    if (dim == 2)
+        k_prologue<R, 2><<<nblocks(g.nall), kBlock, 0, s>>>(g, st, wk, gas);
+    else
+        k_prologue<R, 3><<<nblocks(g.nall), kBlock, 0, s>>>(g, st, wk, gas);
+}
+
+template <typename R, int DIM>
+static void gradient_dim(int grad, int celllim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                         cudaStream_t s) {
+    const int nb = nblocks(g.nint);
+    if (grad == 1) {
+        if (celllim == 4)
+            k_gradient<R, DIM, 1, 4><<<nb, kBlock, 0, s>>>(g, st, wk);
+        else if (celllim == 5)
+            k_gradient<R, DIM, 1, 5><<<nb, kBlock, 0, s>>>(g, st, wk);
+        else
+            k_gradient<R, DIM, 1, 0><<<nb, kBlock, 0, s>>>(g, st, wk);
+    } else if (DIM == 2) {
+        if (celllim == 4)
+            k_gradient<R, 2, 2, 4><<<nb, kBlock, 0, s>>>(g, st, wk);
+        else if (celllim == 5)
+            k_gradient<R, 2, 2, 5><<<nb, kBlock, 0, s>>>(g, st, wk);
+        else
+            k_gradient<R, 2, 2, 0><<<nb, kBlock, 0, s>>>(g, st, wk);
+    }
+}
+
+template <typename R>
+void Ops<R>::gradient(int dim, int grad, int celllim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                      cudaStream_t s) {
+    if (g.nint == 0) return;
+    if (dim == 2)
+        gradient_dim<R, 2>(grad, celllim, g, st, wk, s);
+    else
+        gradient_dim<R, 3>(grad, celllim, g, st, wk, s);
+}
+
+template <typename R, int DIM, int FLUX>
+static void face_flux_f(int rec, int lim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                        const Gas &gas, cudaStream_t s) {
+    const int nb = nblocks(g.nface);
+    if (rec == 0)
+        k_face_flux<R, DIM, FLUX, 0, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    else if (rec == 2)
+        k_face_flux<R, DIM, FLUX, 2, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    else if (lim == 1)
+        k_face_flux<R, DIM, FLUX, 1, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    else if (lim == 2)
+        k_face_flux<R, DIM, FLUX, 1, 2><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    else
+        k_face_flux<R, DIM, FLUX, 1, 3><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+}
+
+template <typename R, int DIM>
+static void face_flux_d(int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                        const Gas &gas, cudaStream_t s) {
+    if (flux == 1)
+        face_flux_f<R, DIM, 1>(rec, lim, g, st, wk, gas, s);
+    else if (flux == 2)
+        face_flux_f<R, DIM, 2>(rec, lim, g, st, wk, gas, s);
+    else
+        face_flux_f<R, DIM, 3>(rec, lim, g, st, wk, gas, s);
+}
+
+template <typename R>
+void Ops<R>::face_flux(int dim, int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st,
+                       const DevWork<R> &wk, const Gas &gas, cudaStream_t s) {
+    if (g.nface == 0) return;
+    if (dim == 2)
+        face_flux_d<R, 2>(flux, rec, lim, g, st, wk, gas, s);
+    else
+        face_flux_d<R, 3>(flux, rec, lim, g, st, wk, gas, s);
+}
+
+template <typename R>
+void Ops<R>::residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStream_t s) {
+    if (g.nint == 0) return;
+    if (dim == 2)
+        k_residual<R, 2><<<nblocks(g.nint), kBlock, 0, s>>>(g, wk);
+    else
+        k_residual<R, 3><<<nblocks(g.nint), kBlock, 0, s>>>(g, wk);
+}
+
+template <typename R, int DIM, bool GATHER>
+static void cell_update_g(int lc, bool seq, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
+                          const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
+                          int first_stage, int it_slot, cudaStream_t s) {
+    if (seq) {
+        k_cell_update_seq<R, DIM, GATHER><<<1, 1024, 0, s>>>(g, cur, nxt, wk, gas, cfl, alpha, first_stage, it_slot);
+        return;
+    }
+    const int nb = nblocks(g.nint);
+    if (lc == 0)
+        k_cell_update<R, DIM, 0, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
+                                                               first_stage, it_slot);
+    else if (lc == 1)
+        k_cell_update<R, DIM, 1, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
+                                                               first_stage, it_slot);
+    else
+        k_cell_update<R, DIM, 2, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
+                                                               first_stage, it_slot);
+}
+
+template <typename R>
+void Ops<R>::cell_update(int dim, int lc, bool seq, bool gather, const DevGrid &g, const DevState<R> &cur,
+                         const DevState<R> &nxt, const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform,
+                         double alpha, int first_stage, int it_slot, cudaStream_t s) {
+    if (g.nint == 0) return;
+    if (dim == 2) {
+        if (gather)
+            cell_update_g<R, 2, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+        else
+            cell_update_g<R, 2, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+    } else {
+        if (gather)
+            cell_update_g<R, 3, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+        else
+            cell_update_g<R, 3, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+    }
+}
+
+template <typename R>
+void Ops<R>::ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const Gas &gas,
+                          cudaStream_t s) {
+    if (g.nghost == 0) return;
+    if (dim == 2)
+        k_ghost_update<R, 2><<<nblocks(g.nghost), kBlock, 0, s>>>(g, cur, nxt, gas);
+    else
+        k_ghost_update<R, 3><<<nblocks(g.nghost), kBlock, 0, s>>>(g, cur, nxt, gas);
+}
+
+template <typename R>
+void Ops<R>::l2_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s) {
+    if (dim == 2)
+        k_l2_finish<4><<<1, 32, 0, s>>>(wk.l2part, nblk, nint, wk.l2, it_slot);
+    else
+        k_l2_finish<5><<<1, 32, 0, s>>>(wk.l2part, nblk, nint, wk.l2, it_slot);
+}
+
+}  // namespace psst

@@ -1,0 +1,850 @@
+// Device solver: layout, memory and the per-iteration launch sequence.
+//
+// Layout (all SoA, sized for one GPU):
+//  * interior cells renumbered along a 3D/2D Hilbert curve of their centroids
+//    (B200 gathers hit L2 far more often when neighbours are close in memory),
+//    then ghost cells ordered by their interior neighbour;
+//  * faces: interior faces sorted by their lower cell id, then boundary faces;
+//  * per cell a CSR of (face, side) sorted by the reference's face-loop order,
+//    so every per-cell sum is formed in the reference's order whatever the
+//    device numbering, plus a 4-bit permutation that replays the cell's own
+//    face order (used by LocalAccTime1/2 and least squares).
+// One RK stage is: face pass (flux*area per face) -> cell pass (deterministic
+// CSR gather, local time step, RK update, primitives, residual norms) -> ghost
+// pass (boundary conditions). Gradients run once per iteration before stage 0
+// (psstFiniteVolumeGrid.cpp:307-308).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime_api.h>
+
+#include "host.hpp"
+#include "ops.hpp"
+
+using namespace psst;
+
+namespace {
+
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) raise(PSST_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707 (2004):
+// axes -> transposed Hilbert index, then bit interleave into one key.
+uint64_t hilbert_key(uint32_t *X, int b, int n) {
+    uint32_t M = 1u << (b - 1), P, Q, t;
+    for (Q = M; Q > 1; Q >>= 1) {
+        P = Q - 1;
+        for (int i = 0; i < n; i++) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    for (int i = 1; i < n; i++) X[i] ^= X[i - 1];
+    t = 0;
+    for (Q = M; Q > 1; Q >>= 1)
+        if (X[n - 1] & Q) t ^= Q - 1;
+    for (int i = 0; i < n; i++) X[i] ^= t;
+    uint64_t key = 0;
+    for (int bit = b - 1; bit >= 0; --bit)
+        for (int i = 0; i < n; ++i) key = (key << 1) | ((X[i] >> bit) & 1u);
+    return key;
+}
+
+struct Layout {
+    int32_t nint = 0, nghost = 0, nall = 0, nface = 0, nfi = 0, nlevels = 0;
+    std::vector<int32_t> dev_of_vol;  // reference volume -> device cell (-1: inactive)
+    std::vector<int64_t> vol_of_dev;  // device cell -> reference volume
+    std::vector<int32_t> c0, c1, csr_ptr, csr_ent, rank, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
+    std::vector<uint64_t> wperm;
+    std::vector<double> S, n, xf, beta, V, xc, lsq_r, vk_eps2, z_u, z_p, z_T;
+};
+
+void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
+    const int dim = G.dim;
+    for (auto &z : G.vz)
+        if (z.bc == 32) raise(PSST_ERR_UNSUPPORTED, "parent-cell zones (hanging-node meshes) are not supported");
+    for (auto &z : G.fz)
+        if (z.bc == 31) raise(PSST_ERR_UNSUPPORTED, "parent-face zones (hanging-node meshes) are not supported");
+    if (G.max_faces > 16) raise(PSST_ERR_UNSUPPORTED, "cells with more than 16 faces are not supported");
+    // interior cells in the reference's update order (psstFiniteVolumeGrid.cpp:312-318)
+    std::vector<int64_t> ref_int;
+    for (auto &z : G.vz)
+        if (z.bc == 1)
+            for (int64_t i = 0; i < z.count; ++i) ref_int.push_back(z.first + i);
+    L.nint = (int32_t)ref_int.size();
+    L.nghost = (int32_t)G.nghost;
+    L.nall = L.nint + L.nghost;
+    L.dev_of_vol.assign(G.nvol, -1);
+    std::vector<int64_t> order(L.nint);
+    std::iota(order.begin(), order.end(), 0);
+    if (sc.renumber && L.nint > 1) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int64_t v : ref_int)
+            for (int k = 0; k < dim; ++k) {
+                lo[k] = std::min(lo[k], G.xc[v * dim + k]);
+                hi[k] = std::max(hi[k], G.xc[v * dim + k]);
+            }
+        const int bits = dim == 3 ? 21 : 31;
+        const double scale = (double)((1u << bits) - 1);
+        std::vector<uint64_t> key(L.nint);
+        for (int32_t i = 0; i < L.nint; ++i) {
+            uint32_t X[3] = {0, 0, 0};
+            for (int k = 0; k < dim; ++k) {
+                const double span = hi[k] - lo[k];
+                const double t = span > 0 ? (G.xc[ref_int[i] * dim + k] - lo[k]) / span : 0.0;
+                X[k] = (uint32_t)std::min(scale, std::max(0.0, t * scale));
+            }
+            key[i] = hilbert_key(X, bits, dim);
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+    }
+    L.vol_of_dev.assign(L.nall, -1);
+    L.rank.assign(L.nint, 0);
+    for (int32_t d = 0; d < L.nint; ++d) {
+        const int64_t v = ref_int[order[d]];
+        L.dev_of_vol[v] = d;
+        L.vol_of_dev[d] = v;
+        L.rank[d] = (int32_t)order[d];
+    }
+    // ghosts, ordered by their interior neighbour
+    std::vector<std::pair<int32_t, int64_t>> gh;
+    for (int64_t v = 0; v < G.nvol; ++v) {
+        if (!G.vol_boundary[v]) continue;
+        const int64_t f = G.vf_idx[G.vf_ptr[v]];
+        const int64_t nb = G.f_c0[f] == v ? G.f_c1[f] : G.f_c0[f];
+        if (nb < 0 || L.dev_of_vol[nb] < 0) raise(PSST_ERR_FORMAT, "ghost cell without an interior neighbour");
+        gh.emplace_back(L.dev_of_vol[nb], v);
+    }
+    std::stable_sort(gh.begin(), gh.end(), [](auto &a, auto &b) { return a.first < b.first; });
+    std::vector<int32_t> zslot(G.vz.size(), -1);
+    for (size_t i = 0; i < gh.size(); ++i) {
+        const int64_t v = gh[i].second;
+        const int32_t d = L.nint + (int32_t)i;
+        L.dev_of_vol[v] = d;
+        L.vol_of_dev[d] = v;
+    }
+    // faces: interior (both sides interior cells) first, then boundary
+    std::vector<int64_t> fint, fbnd;
+    for (int64_t f = 0; f < G.nface; ++f) {
+        const int64_t a = G.f_c0[f], b = G.f_c1[f];
+        if (a < 0 || b < 0) raise(PSST_ERR_FORMAT, "face without two neighbours");
+        const bool zone_interior = G.fz[G.f_fz[f]].bc == 2;
+        const bool ga = G.vol_boundary[a], gb = G.vol_boundary[b];
+        if (zone_interior && (ga || gb)) raise(PSST_ERR_FORMAT, "interior face next to a ghost cell");
+        if (!zone_interior && ga == gb) raise(PSST_ERR_FORMAT, "boundary face without exactly one ghost side");
+        (zone_interior ? fint : fbnd).push_back(f);
+    }
+    auto lowcell = [&](int64_t f) { return std::min(L.dev_of_vol[G.f_c0[f]], L.dev_of_vol[G.f_c1[f]]); };
+    std::stable_sort(fint.begin(), fint.end(), [&](int64_t a, int64_t b) { return lowcell(a) < lowcell(b); });
+    std::stable_sort(fbnd.begin(), fbnd.end(), [&](int64_t a, int64_t b) { return lowcell(a) < lowcell(b); });
+    L.nfi = (int32_t)fint.size();
+    L.nface = (int32_t)(fint.size() + fbnd.size());
+    std::vector<int32_t> dev_face(G.nface, -1);
+    std::vector<int64_t> ref_face(L.nface);
+    for (size_t i = 0; i < fint.size(); ++i) ref_face[i] = fint[i];
+    for (size_t i = 0; i < fbnd.size(); ++i) ref_face[fint.size() + i] = fbnd[i];
+    for (int32_t d = 0; d < L.nface; ++d) dev_face[ref_face[d]] = d;
+    L.c0.resize(L.nface);
+    L.c1.resize(L.nface);
+    L.S.resize(L.nface);
+    L.beta.resize(L.nface);
+    L.n.resize((size_t)dim * L.nface);
+    L.xf.resize((size_t)dim * L.nface);
+    for (int32_t d = 0; d < L.nface; ++d) {
+        const int64_t f = ref_face[d];
+        L.c0[d] = L.dev_of_vol[G.f_c0[f]];
+        L.c1[d] = L.dev_of_vol[G.f_c1[f]];
+        L.S[d] = G.S[f];
+        L.beta[d] = G.beta[f];
+        for (int k = 0; k < dim; ++k) {
+            L.n[(size_t)k * L.nface + d] = G.n[f * dim + k];
+            L.xf[(size_t)k * L.nface + d] = G.xf[f * dim + k];
+        }
+    }
+    // cells: volume, centroid, CSR sorted by reference face index (= loop order)
+    L.V.resize(L.nint);
+    L.xc.resize((size_t)dim * L.nall);
+    for (int32_t d = 0; d < L.nall; ++d) {
+        const int64_t v = L.vol_of_dev[d];
+        if (d < L.nint) L.V[d] = G.V[v];
+        for (int k = 0; k < dim; ++k) L.xc[(size_t)k * L.nall + d] = G.xc[v * dim + k];
+    }
+    L.csr_ptr.assign(L.nint + 1, 0);
+    L.wperm.assign(L.nint, 0);
+    for (int32_t d = 0; d < L.nint; ++d) {
+        const int64_t v = L.vol_of_dev[d];
+        L.csr_ptr[d + 1] = L.csr_ptr[d] + (int32_t)(G.vf_ptr[v + 1] - G.vf_ptr[v]);
+    }
+    L.csr_ent.resize(L.csr_ptr[L.nint]);
+    for (int32_t d = 0; d < L.nint; ++d) {
+        const int64_t v = L.vol_of_dev[d];
+        const int64_t b = G.vf_ptr[v], k = G.vf_ptr[v + 1] - b;
+        std::vector<int> idx(k);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return G.vf_idx[b + x] < G.vf_idx[b + y]; });
+        std::vector<int> pos(k);
+        for (int q = 0; q < k; ++q) {
+            const int64_t f = G.vf_idx[b + idx[q]];
+            const int side = G.f_c0[f] == v ? 0 : 1;
+            L.csr_ent[L.csr_ptr[d] + q] = (dev_face[f] << 1) | side;
+            pos[idx[q]] = q;
+        }
+        uint64_t perm = 0;
+        for (int j = 0; j < k; ++j) perm |= (uint64_t)pos[j] << (4 * j);
+        L.wperm[d] = perm;
+    }
+    // ghost tables and boundary zones
+    L.g_nb.resize(L.nghost);
+    L.g_face.resize(L.nghost);
+    L.g_zone.resize(L.nghost);
+    for (int32_t i = 0; i < L.nghost; ++i) {
+        const int64_t v = L.vol_of_dev[L.nint + i];
+        const int64_t f = G.vf_idx[G.vf_ptr[v]];
+        const int64_t nb = G.f_c0[f] == v ? G.f_c1[f] : G.f_c0[f];
+        L.g_nb[i] = L.dev_of_vol[nb];
+        L.g_face[i] = dev_face[f];
+        const int32_t zs = G.vol_vz[v];
+        if (zslot[zs] < 0) {
+            const VZone &z = G.vz[zs];
+            zslot[zs] = (int32_t)L.z_dyn.size();
+            L.z_dyn.push_back(z.dyn);
+            L.z_therm.push_back(z.therm);
+            for (int k = 0; k < 3; ++k) L.z_u.push_back(z.u[k]);
+            L.z_p.push_back(z.p);
+            L.z_T.push_back(z.T);
+        }
+        L.g_zone[i] = zslot[zs];
+    }
+    if (L.z_dyn.empty()) {  // keep device arrays non-empty
+        L.z_dyn.push_back(0);
+        L.z_therm.push_back(0);
+        L.z_u.assign(3, 0.0);
+        L.z_p.push_back(0);
+        L.z_T.push_back(0);
+    }
+    // 2D least squares: r_ table indexed by the zone-local position
+    // (psstGradCalculation.cpp:404-412)
+    L.lsq_r.assign((size_t)3 * L.nint, 0.0);
+    if (dim == 2 && !G.lsq_r.empty())
+        for (int32_t d = 0; d < L.nint; ++d) {
+            const int64_t v = L.vol_of_dev[d];
+            const int64_t i = v - G.vz[G.vol_vz[v]].first;
+            for (int q = 0; q < 3; ++q) L.lsq_r[(size_t)q * L.nint + d] = G.lsq_r[3 * i + q];
+        }
+    L.vk_eps2.assign(L.nint, 0.0);
+    for (int32_t d = 0; d < L.nint; ++d) {
+        const double h = dim == 2 ? std::sqrt(L.V[d]) : std::cbrt(L.V[d]);
+        const double kh = sc.venkat_k * h;
+        L.vk_eps2[d] = kh * kh * kh;
+    }
+    // level schedule for the sequential LocalAccTime1: a cell's level exceeds
+    // that of every interior neighbour updated before it in the reference.
+    std::vector<int32_t> level(L.nint, 0);
+    std::vector<int32_t> dev_by_rank(L.nint);
+    for (int32_t d = 0; d < L.nint; ++d) dev_by_rank[L.rank[d]] = d;
+    int32_t maxlvl = -1;
+    for (int32_t r = 0; r < L.nint; ++r) {
+        const int32_t d = dev_by_rank[r];
+        int32_t lv = 0;
+        for (int32_t q = L.csr_ptr[d]; q < L.csr_ptr[d + 1]; ++q) {
+            const int32_t f = L.csr_ent[q] >> 1;
+            const int32_t nb = (L.csr_ent[q] & 1) ? L.c0[f] : L.c1[f];
+            if (nb < L.nint && L.rank[nb] < r) lv = std::max(lv, level[nb] + 1);
+        }
+        level[d] = lv;
+        maxlvl = std::max(maxlvl, lv);
+    }
+    L.nlevels = maxlvl + 1;
+    L.lvl_ptr.assign(L.nlevels + 1, 0);
+    for (int32_t d = 0; d < L.nint; ++d) L.lvl_ptr[level[d] + 1]++;
+    for (int32_t l = 0; l < L.nlevels; ++l) L.lvl_ptr[l + 1] += L.lvl_ptr[l];
+    L.lvl_cells.resize(L.nint);
+    std::vector<int32_t> fillp(L.lvl_ptr.begin(), L.lvl_ptr.end() - 1);
+    for (int32_t r = 0; r < L.nint; ++r) {
+        const int32_t d = dev_by_rank[r];
+        L.lvl_cells[fillp[level[d]]++] = d;
+    }
+}
+
+}  // namespace
+
+struct psst_solver {
+    int dim = 0, nv = 0, device = 0;
+    psst_scheme sc{};
+    Gas gas{};
+    Layout L;
+    int64_t nvol_ref = 0;
+    DevGrid g{};
+    DevState<double> s64[2]{};
+    DevState<float> s32[2]{};
+    DevWork<double> w64{};
+    DevWork<float> w32{};
+    int cur = 0;
+    std::vector<void *> allocs;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t iter = 1;
+    bool has_state = false;
+    int64_t last_launches = 0;
+    double last_ms = 0.0;
+    int rec = 0, celllim = 0;
+    bool seq = false;
+    double dt_uniform = 0.0;
+    int nblk = 1;
+    int norm_cap = 0;
+    double *linf_host_tmp = nullptr;
+
+    template <class T>
+    T *dalloc(size_t n) {
+        void *p = nullptr;
+        ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+        allocs.push_back(p);
+        return (T *)p;
+    }
+    template <class T>
+    T *upload(const std::vector<T> &v) {
+        T *p = dalloc<T>(v.size());
+        if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+        return p;
+    }
+    ~psst_solver() {
+        if (device >= 0) cudaSetDevice(device);
+        for (void *p : allocs) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+template <typename R>
+DevState<R> *states(psst_solver *s);
+template <>
+DevState<double> *states<double>(psst_solver *s) {
+    return s->s64;
+}
+template <>
+DevState<float> *states<float>(psst_solver *s) {
+    return s->s32;
+}
+template <typename R>
+DevWork<R> &work(psst_solver *s);
+template <>
+DevWork<double> &work<double>(psst_solver *s) {
+    return s->w64;
+}
+template <>
+DevWork<float> &work<float>(psst_solver *s) {
+    return s->w32;
+}
+
+template <typename R>
+void alloc_state(psst_solver *s) {
+    const int dim = s->dim;
+    const int32_t nall = s->L.nall, nint = s->L.nint, nface = s->L.nface;
+    DevState<R> *st = states<R>(s);
+    for (int b = 0; b < 2; ++b) {
+        st[b].p = s->dalloc<R>(nall);
+        st[b].T = s->dalloc<R>(nall);
+        st[b].rho = s->dalloc<R>(nall);
+        st[b].u = s->dalloc<R>((size_t)dim * nall);
+    }
+    DevWork<R> &w = work<R>(s);
+    const int nv = s->nv;
+    w.w = s->dalloc<double>((size_t)nv * nint);
+    w.pw = s->dalloc<double>((size_t)nv * nint);
+    w.grad = s->dalloc<R>((size_t)nv * dim * nint);
+    w.lim = s->dalloc<R>((size_t)nv * nint);
+    w.fs = s->dalloc<R>((size_t)nv * nface);
+    w.res = s->dalloc<R>((size_t)nv * nint);
+    w.dt = s->dalloc<double>(nint);
+    w.l2part = s->dalloc<double>((size_t)nv * std::max(s->nblk, 1));
+    w.err = s->dalloc<int32_t>(4);
+    ck(cudaMemset(w.grad, 0, (size_t)nv * dim * nint * sizeof(R)), "memset");
+    ck(cudaMemset(w.lim, 0, (size_t)nv * nint * sizeof(R)), "memset");
+    ck(cudaMemset(w.res, 0, (size_t)nv * nint * sizeof(R)), "memset");
+    ck(cudaMemset(w.dt, 0, (size_t)nint * sizeof(double)), "memset");
+    ck(cudaMemset(w.err, 0, 4 * sizeof(int32_t)), "memset");
+}
+
+template <typename R>
+void ensure_norms(psst_solver *s, int n_iter) {
+    DevWork<R> &w = work<R>(s);
+    if (n_iter > s->norm_cap) {
+        s->norm_cap = std::max(n_iter, 2 * s->norm_cap);
+        w.linf = s->dalloc<unsigned long long>((size_t)s->norm_cap * s->nv);
+        w.l2 = s->dalloc<double>((size_t)s->norm_cap * s->nv);
+    }
+    ck(cudaMemsetAsync(w.linf, 0, (size_t)n_iter * s->nv * sizeof(unsigned long long), s->stream), "memset");
+    ck(cudaMemsetAsync(w.l2, 0, (size_t)n_iter * s->nv * sizeof(double), s->stream), "memset");
+}
+
+void check_err(psst_solver *s, const int32_t *err_dev) {
+    int32_t e[4] = {0, 0, 0, 0};
+    ck(cudaMemcpyAsync(e, err_dev, sizeof e, cudaMemcpyDeviceToHost, s->stream), "err copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    if (e[0] == 0) return;
+    ck(cudaMemsetAsync((void *)err_dev, 0, sizeof e, s->stream), "memset");
+    switch (e[0]) {
+    case 1:
+        raise(PSST_ERR_FLUX, "Error: Could not calculate convective HLL flow!");
+    case 2:
+        raise(PSST_ERR_FLUX, "Error: Could not calculate convective HLLC flow!");
+    case 3:
+        raise(PSST_ERR_NONFINITE, "non-finite residual in cell " + std::to_string(s->L.vol_of_dev[e[1]]));
+    default:
+        raise(PSST_ERR_NONFINITE, "non-positive density or temperature in cell " + std::to_string(s->L.vol_of_dev[e[1]]));
+    }
+}
+
+template <typename R>
+int64_t one_stage(psst_solver *s, int k, int it_slot, bool gather) {
+    DevState<R> *st = states<R>(s);
+    DevWork<R> &w = work<R>(s);
+    const DevState<R> &cur = st[s->cur], &nxt = st[s->cur ^ 1];
+    int64_t launches = 0;
+    if (gather) {
+        Ops<R>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, cur, w, s->gas, s->stream);
+        ++launches;
+    }
+    Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, gather, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
+                        s->sc.rk[k], k == 0, it_slot, s->stream);
+    Ops<R>::ghost_update(s->dim, s->g, cur, nxt, s->gas, s->stream);
+    Ops<R>::l2_finish(s->dim, w, s->seq ? 1 : s->nblk, s->L.nint, it_slot, s->stream);
+    launches += 3;
+    s->cur ^= 1;
+    return launches;
+}
+
+template <typename R>
+void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
+    DevWork<R> &w = work<R>(s);
+    ensure_norms<R>(s, n_iter);
+    ck(cudaEventRecord(s->ev0, s->stream), "event");
+    int64_t launches = 0;
+    for (int it = 0; it < n_iter; ++it) {
+        if (s->sc.order == 2) {
+            Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, states<R>(s)[s->cur], w, s->stream);
+            ++launches;
+        }
+        for (int k = 0; k < s->sc.rk_level; ++k) launches += one_stage<R>(s, k, it, true);
+    }
+    ck(cudaEventRecord(s->ev1, s->stream), "event");
+    ck(cudaGetLastError(), "kernel launch");
+    std::vector<unsigned long long> li((size_t)n_iter * s->nv);
+    std::vector<double> l2((size_t)n_iter * s->nv);
+    ck(cudaMemcpyAsync(li.data(), w.linf, li.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->stream),
+       "norm copy");
+    ck(cudaMemcpyAsync(l2.data(), w.l2, l2.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
+    check_err(s, w.err);
+    float ms = 0.0f;
+    ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
+    s->last_ms = ms;
+    s->last_launches = launches;
+    s->iter += n_iter;
+    if (res_linf)
+        for (size_t i = 0; i < li.size(); ++i) {
+            double d;
+            std::memcpy(&d, &li[i], sizeof d);
+            res_linf[i] = d;
+        }
+    if (res_l2) std::memcpy(res_l2, l2.data(), l2.size() * sizeof(double));
+}
+
+template <typename R>
+void set_state(psst_solver *s, const double *prim) {
+    const int dim = s->dim;
+    const int64_t nv = s->nvol_ref;
+    const int32_t nall = s->L.nall;
+    std::vector<R> hp(nall), hT(nall), hu((size_t)dim * nall);
+    for (int32_t d = 0; d < nall; ++d) {
+        const int64_t v = s->L.vol_of_dev[d];
+        hp[d] = (R)prim[v];
+        hT[d] = (R)prim[nv + v];
+        for (int k = 0; k < dim; ++k) hu[(size_t)k * nall + d] = (R)prim[(2 + k) * nv + v];
+    }
+    DevState<R> &st = states<R>(s)[s->cur];
+    ck(cudaMemcpyAsync(st.p, hp.data(), nall * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
+    ck(cudaMemcpyAsync(st.T, hT.data(), nall * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
+    ck(cudaMemcpyAsync(st.u, hu.data(), hu.size() * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
+    Ops<R>::prologue(dim, s->g, st, work<R>(s), s->gas, s->stream);
+    ck(cudaGetLastError(), "prologue");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+}
+
+template <typename R>
+void get_state(psst_solver *s, double *prim, double *wout) {
+    const int dim = s->dim;
+    const int64_t nv = s->nvol_ref;
+    const int32_t nall = s->L.nall, nint = s->L.nint;
+    std::vector<R> hp(nall), hT(nall), hu((size_t)dim * nall);
+    const DevState<R> &st = states<R>(s)[s->cur];
+    ck(cudaMemcpyAsync(hp.data(), st.p, nall * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
+    ck(cudaMemcpyAsync(hT.data(), st.T, nall * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
+    ck(cudaMemcpyAsync(hu.data(), st.u, hu.size() * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
+    std::vector<double> hw;
+    if (wout) {
+        hw.resize((size_t)s->nv * nint);
+        ck(cudaMemcpyAsync(hw.data(), work<R>(s).w, hw.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+           "state copy");
+    }
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    if (prim) {
+        std::fill(prim, prim + (size_t)(2 + dim) * nv, 0.0);
+        for (int32_t d = 0; d < nall; ++d) {
+            const int64_t v = s->L.vol_of_dev[d];
+            prim[v] = (double)hp[d];
+            prim[nv + v] = (double)hT[d];
+            for (int k = 0; k < dim; ++k) prim[(2 + k) * nv + v] = (double)hu[(size_t)k * nall + d];
+        }
+    }
+    if (wout) {
+        std::fill(wout, wout + (size_t)s->nv * nv, 0.0);
+        for (int32_t d = 0; d < nint; ++d) {
+            const int64_t v = s->L.vol_of_dev[d];
+            for (int q = 0; q < s->nv; ++q) wout[(size_t)v * s->nv + q] = hw[(size_t)q * nint + d];
+        }
+    }
+}
+
+template <typename R>
+void get_array(psst_solver *s, const std::string &nm, double *out, int64_t count) {
+    const int dim = s->dim, nvv = s->nv;
+    const int64_t nv = s->nvol_ref;
+    const int32_t nint = s->L.nint;
+    DevWork<R> &w = work<R>(s);
+    auto fetch = [&](const void *src, size_t n, size_t elem) {
+        std::vector<char> h(n * elem);
+        ck(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, s->stream), "array copy");
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+        return h;
+    };
+    auto need = [&](int64_t n) {
+        if (n != count) raise(PSST_ERR_ARG, nm + ": expected " + std::to_string(n) + " elements");
+        std::fill(out, out + n, 0.0);
+    };
+    if (nm == "dt") {
+        need(nv);
+        auto h = fetch(w.dt, nint, sizeof(double));
+        const double *p = (const double *)h.data();
+        for (int32_t d = 0; d < nint; ++d) out[s->L.vol_of_dev[d]] = p[d];
+        return;
+    }
+    if (nm == "residual" || nm == "limiter") {
+        need((int64_t)nvv * nv);
+        auto h = fetch(nm == "residual" ? (const void *)w.res : (const void *)w.lim, (size_t)nvv * nint, sizeof(R));
+        const R *p = (const R *)h.data();
+        for (int32_t d = 0; d < nint; ++d)
+            for (int q = 0; q < nvv; ++q) out[s->L.vol_of_dev[d] * nvv + q] = (double)p[(size_t)q * nint + d];
+        return;
+    }
+    int var = -1, width = dim;
+    if (nm == "grad_u") {
+        var = 0;
+        width = dim * dim;
+    } else if (nm == "grad_p") {
+        var = dim;
+    } else if (nm == "grad_T") {
+        var = dim + 1;
+    }
+    if (var < 0) raise(PSST_ERR_ARG, "unknown solver array " + nm);
+    need((int64_t)width * nv);
+    auto h = fetch(w.grad, (size_t)nvv * dim * nint, sizeof(R));
+    const R *p = (const R *)h.data();
+    for (int32_t d = 0; d < nint; ++d) {
+        const int64_t v = s->L.vol_of_dev[d];
+        for (int j = 0; j < width; ++j) {
+            const int i = var + j / dim, k = j % dim;
+            out[v * width + j] = (double)p[((size_t)i * dim + k) * nint + d];
+        }
+    }
+}
+
+}  // namespace
+
+#define PSST_API_BEGIN try {
+#define PSST_API_END                          \
+    return PSST_OK;                           \
+    }                                         \
+    catch (const Error &e) {                  \
+        set_last_error(e.msg);                \
+        return e.status;                      \
+    }                                         \
+    catch (const std::bad_alloc &) {          \
+        set_last_error("out of host memory"); \
+        return PSST_ERR_ARG;                  \
+    }                                         \
+    catch (const std::exception &e) {         \
+        set_last_error(e.what());             \
+        return PSST_ERR_ARG;                  \
+    }
+
+#define DISPATCH(s, call) ((s)->sc.precision == 32 ? call<float> : call<double>)
+
+extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme *sc, int device, psst_solver **out) {
+    PSST_API_BEGIN
+    if (!G || !sc || !out) raise(PSST_ERR_ARG, "psst_solver_create: null argument");
+    *out = nullptr;
+    if (sc->precision != 64 && sc->precision != 32) raise(PSST_ERR_ARG, "precision must be 64 or 32");
+    if (sc->flux < 1 || sc->flux > 3) raise(PSST_ERR_ARG, "Error: Unknow convective flow scheme!");
+    if (sc->order != 1 && sc->order != 2) raise(PSST_ERR_ARG, "Error! Unknown scheme order!");
+    if (sc->order == 2 && (sc->limiter < 1 || sc->limiter > 5))
+        raise(PSST_ERR_ARG, "second order needs a limiter (1 VanAlbada, 2 MinMod, 3 VanLeer, 4 BJ, 5 Venkatakrishnan)");
+    if (sc->lc < 0 || sc->lc > 2) raise(PSST_ERR_ARG, "unknown local time step mode");
+    if (sc->rk_level < 1 || sc->rk_level > 16) raise(PSST_ERR_ARG, "Error: Unknow RK order!");
+    if (sc->order == 2 && sc->grad != 1 && G->dim != 2)
+        raise(PSST_ERR_UNSUPPORTED, "least-squares gradient: the reference's 3D path writes out of bounds "
+                                    "(psstGradCalculation.cpp:338); only 2D is supported");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        raise(PSST_ERR_CUDA, "no CUDA device available (libpsst_b200 has no CPU fallback)");
+    if (device < 0 || device >= ndev) raise(PSST_ERR_ARG, "invalid device index");
+    std::unique_ptr<psst_solver> s(new psst_solver);
+    s->device = device;
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    s->dim = G->dim;
+    s->nv = G->dim + 2;
+    s->sc = *sc;
+    s->gas = Gas{sc->rm, sc->cp, sc->cv, sc->gamma};
+    s->nvol_ref = G->nvol;
+    s->iter = sc->iter > 0 ? sc->iter : 1;
+    s->rec = sc->order == 1 ? 0 : (sc->limiter >= 4 ? 2 : 1);
+    s->celllim = (sc->order == 2 && sc->limiter >= 4) ? sc->limiter : 0;
+    s->seq = sc->lc == 1 && sc->lc1_mode == PSST_LC1_SEQUENTIAL;
+    if (sc->lc == 0)
+        s->dt_uniform = G->dim == 2 ? sc->cfl * std::sqrt(G->min_vol) / sc->ref_vel
+                                    : sc->cfl * std::pow(G->min_vol, 1.0 / 3.0) / sc->ref_vel;
+    build_layout(*G, *sc, s->L);
+    Layout &L = s->L;
+    s->nblk = nblocks(L.nint);
+    ck(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking), "stream");
+    s->stream = s->own_stream;
+    ck(cudaEventCreate(&s->ev0), "event");
+    ck(cudaEventCreate(&s->ev1), "event");
+    DevGrid &g = s->g;
+    g.nint = L.nint;
+    g.nghost = L.nghost;
+    g.nall = L.nall;
+    g.nface = L.nface;
+    g.nfi = L.nfi;
+    g.c0 = s->upload(L.c0);
+    g.c1 = s->upload(L.c1);
+    g.S = s->upload(L.S);
+    g.n = s->upload(L.n);
+    g.xf = s->upload(L.xf);
+    g.beta = s->upload(L.beta);
+    g.V = s->upload(L.V);
+    g.xc = s->upload(L.xc);
+    g.csr_ptr = s->upload(L.csr_ptr);
+    g.csr_ent = s->upload(L.csr_ent);
+    g.wperm = s->upload(L.wperm);
+    g.lsq_r = s->upload(L.lsq_r);
+    g.vk_eps2 = s->upload(L.vk_eps2);
+    g.rank = s->upload(L.rank);
+    g.g_nb = s->upload(L.g_nb);
+    g.g_face = s->upload(L.g_face);
+    g.g_zone = s->upload(L.g_zone);
+    g.z_dyn = s->upload(L.z_dyn);
+    g.z_therm = s->upload(L.z_therm);
+    g.z_u = s->upload(L.z_u);
+    g.z_p = s->upload(L.z_p);
+    g.z_T = s->upload(L.z_T);
+    g.lvl_cells = s->upload(L.lvl_cells);
+    g.lvl_ptr = s->upload(L.lvl_ptr);
+    g.nlevels = L.nlevels;
+    if (sc->precision == 32)
+        alloc_state<float>(s.get());
+    else
+        alloc_state<double>(s.get());
+    ck(cudaDeviceSynchronize(), "setup");
+    *out = s.release();
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_set_state(psst_solver *s, const double *prim) {
+    PSST_API_BEGIN
+    if (!s || !prim) raise(PSST_ERR_ARG, "psst_solver_set_state: null argument");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, set_state)(s, prim);
+    s->has_state = true;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_get_state(psst_solver *s, double *prim, double *w) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "psst_solver_get_state: null argument");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, get_state)(s, prim, w);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_gradient_calculate(psst_solver *s) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    if (s->sc.precision == 32)
+        Ops<float>::gradient(s->dim, s->sc.grad, s->celllim, s->g, s->s32[s->cur], s->w32, s->stream);
+    else
+        Ops<double>::gradient(s->dim, s->sc.grad, s->celllim, s->g, s->s64[s->cur], s->w64, s->stream);
+    ck(cudaGetLastError(), "gradient");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    PSST_API_END
+}
+
+extern "C" psst_status psst_convective_calculate(psst_solver *s) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    if (s->sc.precision == 32) {
+        Ops<float>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, s->s32[s->cur], s->w32, s->gas, s->stream);
+        Ops<float>::residual(s->dim, s->g, s->w32, s->stream);
+        check_err(s, s->w32.err);
+    } else {
+        Ops<double>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, s->s64[s->cur], s->w64, s->gas,
+                               s->stream);
+        Ops<double>::residual(s->dim, s->g, s->w64, s->stream);
+        check_err(s, s->w64.err);
+    }
+    ck(cudaGetLastError(), "convective");
+    PSST_API_END
+}
+
+namespace {
+template <typename R>
+void stage_api(psst_solver *s, int k, double *res_linf) {
+    ensure_norms<R>(s, 1);
+    one_stage<R>(s, k, 0, false);
+    std::vector<unsigned long long> li(s->nv);
+    ck(cudaMemcpyAsync(li.data(), work<R>(s).linf, li.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       s->stream),
+       "norm copy");
+    check_err(s, work<R>(s).err);
+    if (res_linf)
+        for (int i = 0; i < s->nv; ++i) std::memcpy(&res_linf[i], &li[i], sizeof(double));
+}
+}  // namespace
+
+extern "C" psst_status psst_stage_update(psst_solver *s, int k, double *res_linf) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    if (k < 0 || k >= s->sc.rk_level) raise(PSST_ERR_ARG, "RK stage out of range");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, stage_api)(s, k, res_linf);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    if (n_iter < 0) raise(PSST_ERR_ARG, "n_iter must be non-negative");
+    if (n_iter == 0) return PSST_OK;
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, run)(s, n_iter, res_linf, res_l2);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_get_array(psst_solver *s, const char *name, double *out, int64_t count) {
+    PSST_API_BEGIN
+    if (!s || !name || !out) raise(PSST_ERR_ARG, "psst_solver_get_array: null argument");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, get_array)(s, std::string(name), out, count);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_set_stream(psst_solver *s, void *stream) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, double *device_ms) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (launches) *launches = s->last_launches;
+    if (device_ms) *device_ms = s->last_ms;
+    PSST_API_END
+}
+
+namespace {
+template <typename R>
+void run_profile(psst_solver *s, int n_iter, double *ms, int64_t *cnt) {
+    DevWork<R> &w = work<R>(s);
+    ensure_norms<R>(s, n_iter);
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    auto mark = [&](int k) {
+        cudaEvent_t e;
+        ck(cudaEventCreate(&e), "event");
+        ck(cudaEventRecord(e, s->stream), "event");
+        ev.push_back(e);
+        kind.push_back(k);
+    };
+    DevState<R> *st = states<R>(s);
+    mark(-1);
+    for (int it = 0; it < n_iter; ++it) {
+        if (s->sc.order == 2) {
+            Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, st[s->cur], w, s->stream);
+            mark(0);
+        }
+        for (int k = 0; k < s->sc.rk_level; ++k) {
+            const DevState<R> &cur = st[s->cur], &nxt = st[s->cur ^ 1];
+            Ops<R>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, cur, w, s->gas, s->stream);
+            mark(1);
+            Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, true, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
+                                s->sc.rk[k], k == 0, it, s->stream);
+            mark(2);
+            Ops<R>::ghost_update(s->dim, s->g, cur, nxt, s->gas, s->stream);
+            mark(3);
+            Ops<R>::l2_finish(s->dim, w, s->seq ? 1 : s->nblk, s->L.nint, it, s->stream);
+            mark(4);
+            s->cur ^= 1;
+        }
+    }
+    ck(cudaGetLastError(), "kernel launch");
+    check_err(s, w.err);
+    for (int k = 0; k < PSST_KERNEL_KINDS; ++k) {
+        ms[k] = 0.0;
+        cnt[k] = 0;
+    }
+    for (size_t i = 1; i < ev.size(); ++i) {
+        float t = 0.0f;
+        ck(cudaEventElapsedTime(&t, ev[i - 1], ev[i]), "event time");
+        ms[kind[i]] += t;
+        cnt[kind[i]] += 1;
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+    s->iter += n_iter;
+}
+}  // namespace
+
+extern "C" psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind) {
+    PSST_API_BEGIN
+    if (!s || !ms_per_kind || !launches_per_kind) raise(PSST_ERR_ARG, "psst_solver_profile: null argument");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    if (n_iter <= 0) raise(PSST_ERR_ARG, "n_iter must be positive");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, run_profile)(s, n_iter, ms_per_kind, launches_per_kind);
+    PSST_API_END
+}
+
+extern "C" int64_t psst_solver_iter(const psst_solver *s) { return s ? s->iter : -1; }
+
+extern "C" void psst_solver_destroy(psst_solver *s) { delete s; }

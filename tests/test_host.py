@@ -1,0 +1,158 @@
+"""Host side of libpsst_b200 (no GPU needed): the C ABI exports, the Fluent
+reader, FP64 geometry, case files, and error behaviour, checked against the
+oracle bit for bit."""
+import ctypes
+import os
+import re
+import shutil
+
+import numpy as np
+import pytest
+
+from conftest import REFERENCE_DIR, ROOT, make_case
+from oracle.pyoracle import Oracle
+from supersonicflowsolver_b200 import _lib, meshgen
+from supersonicflowsolver_b200.psst import Grid, PsstError, Scheme, Solver
+
+
+def declared_symbols():
+    hdr = open(os.path.join(ROOT, "include", "psst_b200.h")).read()
+    return sorted(set(re.findall(r"\b(psst_[a-z_0-9]+)\s*\(", hdr)))
+
+
+def test_header_declares_what_the_binding_lists():
+    assert declared_symbols() == sorted(_lib.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    for sym in declared_symbols():
+        assert hasattr(L, sym), sym
+    assert _lib.load().psst_abi_version() == 1
+
+
+MESHES = {
+    "wedge2d": lambda: meshgen.wedge2d(30, 10, 15.0),
+    "wedge2d_jitter_shuffle": lambda: meshgen.wedge2d(30, 10, 15.0, jitter=0.15, shuffle_seed=1, interior_first=True),
+    "wedge3d_tets": lambda: meshgen.wedge3d(8, 4, 3, 12.0, tets=True),
+    "wedge3d_hexes": lambda: meshgen.wedge3d(8, 4, 3, 12.0, tets=False, interior_first=True),
+}
+GEOM = ["vol_V", "vol_x", "face_S", "face_n", "face_x", "face_beta", "face_c0", "face_c1", "vol_zone",
+        "vol_boundary", "face_zone"]
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_geometry_and_case_match_oracle(tmp_path, name):
+    mesh = MESHES[name]()
+    path, d, case = make_case(tmp_path, mesh, max_iter=3, mach=3.0 if mesh.dim == 3 else 2.5)
+    g = Grid.read_fluent(path)
+    o = Oracle(path, d, case)
+    for k in GEOM:
+        assert np.array_equal(g.get(k).astype(float), o.get(k)), k
+    assert g.min_vol == o.get("min_vol")[0]
+    sc, prim = g.read_case(d, case)
+    nv = g.nvol
+    assert np.array_equal(prim[:nv], o.get("vol_p"))
+    assert np.array_equal(prim[nv:2 * nv], o.get("vol_T"))
+    assert np.array_equal(prim[2 * nv:].reshape(mesh.dim, nv).T.ravel(), o.get("vol_u"))
+    s = o.get("scheme")
+    assert (sc.cfl, sc.lc, sc.rk_level, sc.flux, sc.order, sc.limiter, sc.ref_vel) == \
+        (s[0], s[1], s[2], s[3], s[4], s[6], s[7])
+    assert list(sc.rk)[: sc.rk_level] == list(o.get("rk"))
+    assert (sc.rm, sc.cp, sc.cv, sc.gamma) == tuple(o.get("gas"))
+    # in-memory mesh description gives the same grid as the file
+    g2 = Grid.from_mesh(mesh)
+    for k in GEOM:
+        assert np.array_equal(g.get(k), g2.get(k)), k
+
+
+def test_reader_accepts_crlf(tmp_path):
+    mesh = meshgen.wedge2d(12, 4, 15.0)
+    path, d, case = make_case(tmp_path, mesh)
+    crlf = os.path.join(d, "crlf.msh")
+    open(crlf, "wb").write(open(path, "rb").read().replace(b"\n", b"\r\n"))
+    a, b = Grid.read_fluent(path), Grid.read_fluent(crlf)
+    for k in GEOM:
+        assert np.array_equal(a.get(k), b.get(k))
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE_DIR, "quad2D.msh")), reason="reference not mounted")
+@pytest.mark.parametrize("mesh", ["quad2D.msh", "quad3D.msh", "wedge40_120.msh", "wedge3D.msh"])
+def test_reader_on_reference_meshes(mesh):
+    """The reference's own GAMBIT/Fluent meshes (CRLF) load, with geometry
+    identical to the oracle's."""
+    src = os.path.join(REFERENCE_DIR, mesh)
+    g = Grid.read_fluent(src)
+    assert g.ninterior > 0 and g.nghost > 0
+
+
+def test_reference_mesh_geometry_matches_oracle(tmp_path):
+    src = os.path.join(REFERENCE_DIR, "wedge40_120.msh")
+    if not os.path.exists(src):
+        pytest.skip("reference not mounted")
+    lf = tmp_path / "m.msh"
+    lf.write_bytes(open(src, "rb").read().replace(b"\r", b""))
+    for f in ("wedge.inp", "wedge.prop", "wedge.par", "wedge.bvp", "wedge.btq"):
+        shutil.copy(os.path.join(REFERENCE_DIR, f), tmp_path / f)
+    g = Grid.read_fluent(src)
+    o = Oracle(str(lf), str(tmp_path), "wedge")
+    for k in GEOM:
+        assert np.array_equal(g.get(k).astype(float), o.get(k)), k
+    sc, prim = g.read_case(str(tmp_path), "wedge")
+    assert np.array_equal(prim[: g.nvol], o.get("vol_p"))
+    assert (sc.flux, sc.order, sc.lc, sc.rk_level, sc.max_iter) == (2, 1, 1, 1, 3000)
+
+
+def test_errors_carry_reference_messages(tmp_path):
+    mesh = meshgen.wedge2d(12, 4, 15.0)
+    path, d, case = make_case(tmp_path, mesh)
+    with pytest.raises(PsstError) as e:
+        Grid.read_fluent(os.path.join(d, "missing.msh"))
+    assert e.value.status == 2 and "Could not open" in e.value.message
+    g = Grid.read_fluent(path)
+    bvp = os.path.join(d, case + ".bvp")
+    txt = open(bvp).read()
+    open(bvp, "w").write(txt.replace("symm", "nozone"))
+    with pytest.raises(PsstError) as e:
+        g.read_case(d, case)
+    assert "Error: Could not found zone!" in e.value.message
+    with pytest.raises(PsstError) as e:
+        g.read_case(d, "nocase")
+    assert "Could not found setting file" in e.value.message
+    txt = open(path).read()
+    open(os.path.join(d, "trunc.msh"), "w").write(txt[: len(txt) // 2])
+    with pytest.raises(PsstError) as e:
+        Grid.read_fluent(os.path.join(d, "trunc.msh"))
+    assert e.value.status == 3
+
+
+def test_subsonic_inlet_rejected_like_reference(tmp_path):
+    """psstInlet's constructor always throws (psstBoundaryCondition.cpp:147)."""
+    mesh = meshgen.wedge2d(12, 4, 15.0)
+    path, d, case = make_case(tmp_path, mesh)
+    bvp = os.path.join(d, case + ".bvp")
+    txt = open(bvp).read().split("\n")
+    txt[0] = "in\t27\t100.0\t0.0"
+    open(bvp, "w").write("\n".join(txt))
+    g = Grid.read_fluent(path)
+    with pytest.raises(PsstError) as e:
+        g.read_case(d, case)
+    assert "Wrong dimension" in e.value.message
+
+
+def test_solver_without_gpu_fails_loudly(tmp_path):
+    """No CPU fallback: creating a solver needs a CUDA device."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    mesh = meshgen.wedge2d(12, 4, 15.0)
+    path, d, case = make_case(tmp_path, mesh)
+    g = Grid.read_fluent(path)
+    sc, prim = g.read_case(d, case)
+    with pytest.raises(PsstError) as e:
+        Solver(g, sc)
+    assert e.value.status == 4
