@@ -133,19 +133,20 @@ def traffic_model(grid, nnz, kind):
     g = 8 B geometry word, i = 4 B index."""
     nint, ngh, nf = grid.ninterior, grid.nghost, grid.nface
     K = nnz / nint
-    if kind == "face_flux":
-        # per face: c0,c1 (2i) + S (g) + n (3g) + x_f (3g) read, flux*area (5s) written;
-        # per interior cell: p,T,rho,u (6s) + grads (15s) + limiter (5s) + centroid (3g); ghosts 6s
-        return nf * (8 + 8 + 24 + 24 + 20) + nint * (24 + 60 + 20 + 24) + ngh * 24
-    if kind == "cell_update":
-        # per cell: CSR ptr (i) + K entries (i) + own-order perm (8) + V (g) + own T,u (4s)
-        # + w, prev_w (FP64, 2x5x8, a third on stage 0 amortised) + new p,T,rho,u (6s) + dt (g);
-        # per face: flux*area (5s) + S, n for the time step (4g)
-        return nint * (4 + 4 * K + 8 + 8 + 16 + 80 + 10 + 24 + 8) + nf * (20 + 32)
+    if kind == "face":
+        # per face: face record read (64: c0,c1 (2i), S (g), n (3g), two FP32 offset vectors)
+        # and the face output record written (64: flux*area 5s, time-step terms 8s, padding);
+        # per interior cell: state record (32) + gradient/limiter record (80); ghosts: state (32)
+        return nf * (64 + 64) + nint * (32 + 80) + ngh * 32
+    if kind == "cell":
+        # per cell: CSR ptr (i) + K entries (i) + own-order perm (8) + V (g) + w, prev_w (FP64
+        # 2x5x8, a third more on stage 0 amortised) + new state record (32) + dt (g) + ghost ptr
+        # (i); per face: face output record (64); per ghost: record in and out (2x32) + ids (2i)
+        return nint * (4 + 4 * K + 8 + 8 + 90 + 32 + 8 + 4) + nf * 64 + ngh * 72
     if kind == "gradient":
-        # per cell: CSR (i + K i) + perm + V + eps^2 + own p,T,u (5s) + centroid (3g)
-        # + gradients (15s) + limiter (5s) written; per face: beta, S, n, x_f (8g); ghosts 5s
-        return nint * (4 + 4 * K + 8 + 8 + 8 + 20 + 24 + 60 + 20) + nf * 64 + ngh * 20
+        # per cell: CSR (i + K i) + perm + V + eps^2 + own state record (32) + gradient/limiter
+        # record written (80); per face: face record (64) + beta (g); ghosts: state record (32)
+        return nint * (4 + 4 * K + 8 + 8 + 8 + 32 + 80) + nf * 72 + ngh * 32
     if kind == "ghost_update":
         return ngh * (12 + 20 + 20 + 24 + 24)
     return 0
@@ -361,7 +362,7 @@ def run_gpu(args):
             "finite": finite,
         }
         if not args.no_cpu_baseline:
-            cb = cpu_baseline(1, 2, max(1, os.cpu_count() or 1))
+            cb = cpu_baseline(1, 10, max(1, os.cpu_count() or 1))
             line["cpu_baseline"] = cb
         print(json.dumps(line))
     solver.close()

@@ -221,7 +221,9 @@ psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, doub
 /* Runs n_iter iterations like psst_explicit_solve, with a CUDA event pair
  * around every kernel launch, and returns per kernel kind the summed device
  * time (ms) and the launch count. Kinds: 0 gradient (+cell limiter), 1 face
- * flux, 2 cell update, 3 ghost update, 4 residual-norm finish. */
+ * pass (fluxes and time-step terms), 2 cell pass (residual, time step, RK
+ * update; in the parallel modes also ghosts and norms), 3 ghost update, 4
+ * residual-norm finish (the last two only in the sequential mode). */
 #define PSST_KERNEL_KINDS 5
 psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind);
 

@@ -1,9 +1,52 @@
 // Device-side views shared by the host driver (solver.cpp) and the kernels.
 // Plain structs of device pointers, passed to kernels by value.
+//
+// Per-cell and per-face data that kernels gather through an index are stored
+// as 16-byte-aligned records (one or a few 128-bit loads per gather); data
+// read only at the thread's own index stay structure-of-arrays (coalesced).
 #pragma once
 #include <cstdint>
 
 namespace psst {
+
+// Primitive state of a volume: p, T, rho, u0, u1, (u2), padding.
+template <typename R>
+struct alignas(16) CellRec {
+    R v[8];
+};
+enum { RP = 0, RT = 1, RRHO = 2, RU = 3 };
+
+// Gradients of u.., p, T (g[var * DIM + k]) and the cell limiter of each.
+template <typename R, int DIM>
+struct alignas(16) GradRec {
+    R g[(DIM + 2) * DIM];
+    R lim[DIM + 2];
+};
+
+// Face: neighbours (device ids), area, unit normal (FP64: geometry is kept in
+// FP64 on both paths), and the reconstruction offsets: x_f - x_c0 and
+// x_f - x_c1 for cell-limited MUSCL, or x_c0 - x_c1 in o0 for the
+// Darwish-Moukalled reconstruction. Offsets are formed in FP64 on the host
+// and rounded once to R (exact on the FP64 path).
+template <typename R, int DIM>
+struct alignas(16) FaceRec {
+    int32_t c0, c1;
+    double S;
+    double n[DIM];
+    R o0[DIM];
+    R o1[DIM];
+};
+
+// Output of the face pass for one face: flux * area (DIM+2), then the face's
+// local-time-step terms: for LocalAccTime1 the products u0.n and u1.n of the
+// two neighbours' velocities with the normal (DIM each), the mean sound speed
+// and the area; for LocalAccTime2 S |n_k| (DIM). Padded to 16 bytes.
+template <typename R, int DIM>
+struct alignas(16) FaceOut {
+    static constexpr int NV = DIM + 2;
+    static constexpr int Q0 = NV, Q1 = NV + DIM, CN = NV + 2 * DIM, SA = NV + 2 * DIM + 1;
+    R v[DIM == 3 ? 16 : 12];
+};
 
 struct DevGrid {
     int32_t nint;     // interior cells: device ids [0, nint)
@@ -11,19 +54,17 @@ struct DevGrid {
     int32_t nall;     // nint + nghost
     int32_t nface;    // active faces (zone 31 excluded); interior faces first
     int32_t nfi;      // interior faces: device ids [0, nfi)
-    const int32_t *c0, *c1;   // [nface] device cell ids of neighbour 0 / 1
-    const double *S;          // [nface] face area
-    const double *n;          // [dim][nface] unit normal, neighbour 1 -> neighbour 0
-    const double *xf;         // [dim][nface] face centre
+    const void *frec;         // [nface] FaceRec<R, DIM>
     const double *beta;       // [nface] Green-Gauss interpolation weight (reference table)
     const double *V;          // [nint] cell volume
-    const double *xc;         // [dim][nall] centroid (ghost: its face centre)
+    const double *xc;         // [dim][nall] centroid (ghost: its face centre); least squares only
     const int32_t *csr_ptr;   // [nint+1]
     const int32_t *csr_ent;   // face << 1 | side, sorted by the reference's face-loop order
     const uint64_t *wperm;    // [nint] 4-bit slots: k-th face of the cell's own face order
     const double *lsq_r;      // [3][nint] 2D least-squares coefficients (reference table)
     const double *vk_eps2;    // [nint] Venkatakrishnan epsilon^2 = (K h)^3, h = V^(1/dim)
     const int32_t *rank;      // [nint] position in the reference's interior update order
+    const int32_t *gptr;      // [nint+1] ghosts of each interior cell (ghost index space)
     const int32_t *g_nb;      // [nghost] interior neighbour of each ghost
     const int32_t *g_face;    // [nghost] face of each ghost
     const int32_t *g_zone;    // [nghost] boundary zone slot
@@ -37,20 +78,20 @@ struct DevGrid {
 
 template <typename R>
 struct DevState {
-    R *p, *T, *rho, *u;  // [nall], u: [dim][nall]
+    CellRec<R> *rec;  // [nall]
 };
 
 template <typename R>
 struct DevWork {
     double *w, *pw;      // [dim+2][nint] conservative state, previous-stage state
-    R *grad;             // [dim+2][dim][nint] gradients of u.., p, T
-    R *lim;              // [dim+2][nint] cell limiter (limiters 4/5)
-    R *fs;               // [dim+2][nface] flux * area per face
+    void *grec;          // [nint] GradRec<R, DIM>
+    void *fout;          // [nface] FaceOut<R, DIM>, written by the face pass
     R *res;              // [dim+2][nint] residual (stage-by-stage API only)
     double *dt;          // [nint]
-    unsigned long long *linf;  // [n_iter][dim+2] max |res| (bit pattern of a non-negative double)
-    double *l2part;      // [nblocks][dim+2] partial sums of res^2
+    double *linf;        // [n_iter][dim+2] max over stages and cells of |res|
     double *l2;          // [n_iter][dim+2]
+    double *l2part;      // [nblocks][2][dim+2] per-block sum of res^2 and max |res|
+    unsigned int *ticket;  // [1] blocks finished in the current launch
     int32_t *err;        // [4] error word, face id, cell id, code
 };
 

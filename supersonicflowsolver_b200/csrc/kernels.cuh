@@ -11,6 +11,12 @@
 // sorted by it) for residuals and Green-Gauss gradients, and the cell's own face
 // order (the 4-bit permutation wperm) for the local time step and the
 // least-squares gradient.
+//
+// One RK stage (parallel modes) is two launches: k_face (one thread per face:
+// reconstruction + flux, written as a per-face output record together with the
+// face's local-time-step terms) and k_cell (one thread per interior cell:
+// in-order gather of its faces' records, time step, RK update, its ghosts,
+// norms). Each interior face's flux is computed once.
 #pragma once
 #include <cstdint>
 
@@ -20,8 +26,38 @@ namespace psst {
 
 enum ErrCode { ERR_HLL = 1, ERR_HLLC = 2, ERR_NONFINITE_RES = 3, ERR_BAD_STATE = 4 };
 
+constexpr unsigned FULL = 0xffffffffu;
+
 __device__ __forceinline__ void flag_error(int32_t *err, int code, int id) {
     if (atomicCAS(&err[0], 0, code) == 0) err[1] = id;
+}
+
+// 128-bit loads of a 16-byte-aligned record.
+template <typename T>
+__device__ __forceinline__ T ld16(const T *p) {
+    static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
+    union U {
+        T t;
+        int4 v[sizeof(T) / 16];
+        __device__ U() {}
+    } u;
+    const int4 *q = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); ++i) u.v[i] = q[i];
+    return u.t;
+}
+template <typename T>
+__device__ __forceinline__ void st16(T *p, const T &t) {
+    static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
+    union U {
+        T t;
+        int4 v[sizeof(T) / 16];
+        __device__ U() {}
+    } u;
+    u.t = t;
+    int4 *q = reinterpret_cast<int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); ++i) q[i] = u.v[i];
 }
 
 // psstScalarLimiters.cpp:17-93
@@ -37,25 +73,40 @@ __device__ __forceinline__ R limiter_value(R num, R den) {
 }
 
 template <typename R, int DIM>
-struct FaceState {
+struct Prim {
     R p, T, rho, u[DIM];
 };
 
 template <typename R, int DIM>
-__device__ __forceinline__ void load_state(const DevState<R> &s, int32_t nall, int32_t c, FaceState<R, DIM> &o) {
-    o.p = s.p[c];
-    o.T = s.T[c];
-    o.rho = s.rho[c];
+__device__ __forceinline__ Prim<R, DIM> unpack(const CellRec<R> &c) {
+    Prim<R, DIM> o;
+    o.p = c.v[RP];
+    o.T = c.v[RT];
+    o.rho = c.v[RRHO];
 #pragma unroll
-    for (int k = 0; k < DIM; ++k) o.u[k] = s.u[(int64_t)k * nall + c];
+    for (int k = 0; k < DIM; ++k) o.u[k] = c.v[RU + k];
+    return o;
+}
+template <typename R, int DIM>
+__device__ __forceinline__ CellRec<R> pack(R p, R T, R rho, const R *u) {
+    CellRec<R> c;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) c.v[i] = (R)0;
+    c.v[RP] = p;
+    c.v[RT] = T;
+    c.v[RRHO] = rho;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) c.v[RU + k] = u[k];
+    return c;
 }
 
+// variable i of the reconstructed set: u.. (i < DIM), p (DIM), T (DIM+1)
 template <typename R, int DIM>
-__device__ __forceinline__ R state_var(const FaceState<R, DIM> &s, int i) {
+__device__ __forceinline__ R &pvar(Prim<R, DIM> &s, int i) {
     return i < DIM ? s.u[i] : (i == DIM ? s.p : s.T);
 }
 template <typename R, int DIM>
-__device__ __forceinline__ R &state_var_ref(FaceState<R, DIM> &s, int i) {
+__device__ __forceinline__ R pvar(const Prim<R, DIM> &s, int i) {
     return i < DIM ? s.u[i] : (i == DIM ? s.p : s.T);
 }
 
@@ -68,57 +119,69 @@ __device__ __forceinline__ R roe_avg(R lv, R rv, R ld, R rd) {
     return num / den;
 }
 
-// One interior face: reconstruction (REC 0 first order, 1 Darwish-Moukalled
-// with limiter LIM, 2 cell-limited MUSCL) and the Riemann flux FLUX
-// (1 AUSM, 2 HLL, 3 HLLC). Returns false when the wave speeds cannot be
-// ordered (the reference throws there).
+// Physical flux of a ghost state through a boundary face (psstConvectiveFlow.cpp:123-202).
+template <typename R, int DIM>
+__device__ __forceinline__ void boundary_flux(const Prim<R, DIM> &s, const R nn[DIM], const Gas &gas, R flow[DIM + 2]) {
+    R vn = (R)0, vs = (R)0;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        vn += s.u[k] * nn[k];
+        vs += s.u[k] * s.u[k];
+    }
+    const R H = (R)gas.cp * s.T + (R)0.5 * vs;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) flow[k] = s.rho * s.u[k] * vn + s.p * nn[k];
+    flow[DIM] = s.rho * vn;
+    flow[DIM + 1] = s.rho * vn * H;
+}
+
+// One side of the cell-limited MUSCL reconstruction: phi_f = phi_c + psi_c *
+// grad(phi)_c . (x_f - x_c); rho_f = p_f / (R T_f) as in the DM reconstruction.
+template <typename R, int DIM>
+__device__ __forceinline__ void muscl_side(Prim<R, DIM> &r, const GradRec<R, DIM> &gr, const R off[DIM], R rm) {
+#pragma unroll
+    for (int i = 0; i < DIM + 2; ++i) {
+        R d = (R)0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) d += gr.g[i * DIM + k] * off[k];
+        pvar<R, DIM>(r, i) += gr.lim[i] * d;
+    }
+    r.rho = r.p / (rm * r.T);
+}
+
+// Interior face: reconstruction (REC 0 first order, 1 Darwish-Moukalled with
+// limiter LIM, 2 cell-limited MUSCL) and the Riemann flux FLUX (1 AUSM, 2 HLL,
+// 3 HLLC). r[0] is neighbour 0 (c0), r[1] neighbour 1. Returns false when the
+// wave speeds cannot be ordered (the reference throws there).
 template <typename R, int DIM, int FLUX, int REC, int LIM>
-__device__ __forceinline__ bool interior_flux(const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
-                                              const Gas &gas, int32_t f, const R nn[DIM], R flow[DIM + 2]) {
-    const int32_t c0 = g.c0[f], c1 = g.c1[f];
-    FaceState<R, DIM> r[2];
-    load_state<R, DIM>(st, g.nall, c0, r[0]);
-    load_state<R, DIM>(st, g.nall, c1, r[1]);
+__device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R, DIM> *gr0,
+                                              const GradRec<R, DIM> *gr1, const FaceRec<R, DIM> &fr,
+                                              const R nn[DIM], const Gas &gas, R flow[DIM + 2]) {
     const R rm = (R)gas.rm;
     if (REC == 1) {  // psstReconstructorDM::reconstruct_vals (psstValueReconstructor.cpp:70-134)
-        R Rv[DIM];
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) Rv[j] = (R)(g.xc[(int64_t)j * g.nall + c0] - g.xc[(int64_t)j * g.nall + c1]);
 #pragma unroll
         for (int i = 0; i < DIM + 2; ++i) {
             R dl = (R)0, dr = (R)0;
 #pragma unroll
             for (int k = 0; k < DIM; ++k) {
-                dl += wk.grad[((int64_t)i * DIM + k) * g.nint + c1] * Rv[k];
-                dr += wk.grad[((int64_t)i * DIM + k) * g.nint + c0] * Rv[k];
+                dl += gr1->g[i * DIM + k] * fr.o0[k];
+                dr += gr0->g[i * DIM + k] * fr.o0[k];
             }
-            const R v0 = state_var<R, DIM>(r[0], i), v1 = state_var<R, DIM>(r[1], i);
+            const R v0 = pvar<R, DIM>(r[0], i), v1 = pvar<R, DIM>(r[1], i);
             const R vlm = v1 - ((R)2 * dl - (v0 - v1));
             const R vlp = v0;
             const R vrm = v1;
             const R vrp = v0 + ((R)2 * dr - (v0 - v1));
             const R nl = vlp - v1, dnl = v1 - vlm;
             const R nr = vrm - v0, dnr = v0 - vrp;
-            state_var_ref<R, DIM>(r[0], i) += (R)0.5 * limiter_value<LIM, R>(nr, dnr) * dnr;
-            state_var_ref<R, DIM>(r[1], i) += (R)0.5 * limiter_value<LIM, R>(nl, dnl) * dnl;
+            pvar<R, DIM>(r[0], i) += (R)0.5 * limiter_value<LIM, R>(nr, dnr) * dnr;
+            pvar<R, DIM>(r[1], i) += (R)0.5 * limiter_value<LIM, R>(nl, dnl) * dnl;
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) r[j].rho = r[j].p / (rm * r[j].T);
     } else if (REC == 2) {  // cell-limited MUSCL (limiters 4, 5)
-        const int32_t cc[2] = {c0, c1};
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-#pragma unroll
-            for (int i = 0; i < DIM + 2; ++i) {
-                R d = (R)0;
-#pragma unroll
-                for (int k = 0; k < DIM; ++k)
-                    d += wk.grad[((int64_t)i * DIM + k) * g.nint + cc[j]] *
-                         (R)(g.xf[(int64_t)k * g.nface + f] - g.xc[(int64_t)k * g.nall + cc[j]]);
-                state_var_ref<R, DIM>(r[j], i) += wk.lim[(int64_t)i * g.nint + cc[j]] * d;
-            }
-            r[j].rho = r[j].p / (rm * r[j].T);
-        }
+        muscl_side<R, DIM>(r[0], *gr0, fr.o0, rm);
+        muscl_side<R, DIM>(r[1], *gr1, fr.o1, rm);
     }
     const R cp = (R)gas.cp, cv = (R)gas.cv, gamma = (R)gas.gamma;
     R vn[2], a[2], H[2], M[2];
@@ -172,15 +235,15 @@ __device__ __forceinline__ bool interior_flux(const DevGrid &g, const DevState<R
             ps0 = (R)0.25 * r[0].p * (M[0] - (R)1) * (M[0] - (R)1) * ((R)2 + M[0]);
         }
         const R Mf = Ms0 + Ms1, pf = ps0 + ps1;
-        const int sd = Mf > (R)0 ? 1 : 0;
-        const R t = Mf * a[sd] * r[sd].rho;
+        const bool sd = Mf > (R)0;  // upwind side: 1 if Mf > 0
+        const R t = Mf * (sd ? a[1] : a[0]) * (sd ? r[1].rho : r[0].rho);
 #pragma unroll
         for (int j = 0; j < DIM; ++j) {
             const R pfl = pf * nn[j];
-            flow[j] = t * r[sd].u[j] + pfl;
+            flow[j] = t * (sd ? r[1].u[j] : r[0].u[j]) + pfl;
         }
         flow[DIM] = t;
-        flow[DIM + 1] = t * H[sd];
+        flow[DIM + 1] = t * (sd ? H[1] : H[0]);
         return true;
     }
     // Roe-averaged wave speeds (psstConvectiveFlow.cpp:247-266, 531-550)
@@ -224,15 +287,20 @@ __device__ __forceinline__ bool interior_flux(const DevGrid &g, const DevState<R
 #pragma unroll
         for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[1][j];
     } else if ((s1 <= (R)0 && sh >= (R)0) || (sh <= (R)0 && s0 >= (R)0)) {
-        const int sd = (s1 <= (R)0 && sh >= (R)0) ? 1 : 0;
+        const bool sd = (s1 <= (R)0 && sh >= (R)0);  // star state of side 1, else side 0
         const R ss = sd ? s1 : s0;
         const R tt = ss - sh;
-        const R pr = r[sd].p, dd = r[sd].rho, vv = vn[sd];
+        const R pr = sd ? r[1].p : r[0].p, dd = sd ? r[1].rho : r[0].rho, vv = sd ? vn[1] : vn[0];
 #pragma unroll
-        for (int j = 0; j < DIM; ++j)
-            flow[j] = (sh * (ss * wi[sd][j] - fi[sd][j]) + ss * (pr + dd * (ss - vv) * (sh - vv)) * nn[j]) / tt;
-        flow[DIM] = (sh * (ss * wi[sd][DIM] - fi[sd][DIM])) / tt;
-        flow[DIM + 1] = (sh * (ss * wi[sd][DIM + 1] - fi[sd][DIM + 1]) + ss * (pr + dd * (ss - vv) * (sh - vv)) * sh) / tt;
+        for (int j = 0; j < DIM + 2; ++j) {
+            const R wj = sd ? wi[1][j] : wi[0][j], fj = sd ? fi[1][j] : fi[0][j];
+            if (j < DIM)
+                flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * nn[j]) / tt;
+            else if (j == DIM)
+                flow[j] = (sh * (ss * wj - fj)) / tt;
+            else
+                flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * sh) / tt;
+        }
     } else if (s0 <= (R)0) {
 #pragma unroll
         for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[0][j];
@@ -242,93 +310,123 @@ __device__ __forceinline__ bool interior_flux(const DevGrid &g, const DevState<R
     return true;
 }
 
-// Face pass: flux * area for every active face (interior faces first, then
-// boundary faces whose flux is the physical flux of the ghost state,
-// psstConvectiveFlow.cpp:123-202). Output fs[v][f].
-template <typename R, int DIM, int FLUX, int REC, int LIM>
-__global__ void __launch_bounds__(256) k_face_flux(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
+// ---------------------------------------------------------------------------
+// face pass
+// ---------------------------------------------------------------------------
+
+// One thread per face: reconstruction + Riemann flux (or the ghost's physical
+// flux on boundary faces, psstConvectiveFlow.cpp:123-202), written as
+// flux * area, plus the face's local-time-step terms so that the cell pass
+// needs neither face geometry nor neighbour states:
+//  LocalAccTime1 (psstLocalTimeCalculation.cpp:117-127): u0.n and u1.n per
+//   component, the mean sound speed (sqrt(g R T1) + sqrt(g R T0)) / 2 (the
+//   reference adds the two sound speeds in the opposite order on the other
+//   side; IEEE addition is commutative) and S;
+//  LocalAccTime2 (:189-193): S |n_k|.
+template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
+__global__ void __launch_bounds__(256) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
+    using FO = FaceOut<R, DIM>;
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
+    const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
     R nn[DIM];
 #pragma unroll
-    for (int k = 0; k < DIM; ++k) nn[k] = (R)g.n[(int64_t)k * g.nface + f];
-    const R S = (R)g.S[f];
+    for (int k = 0; k < DIM; ++k) nn[k] = (R)fr.n[k];
+    const R S = (R)fr.S;
+    const Prim<R, DIM> p0 = unpack<R, DIM>(ld16(st.rec + fr.c0));
+    const Prim<R, DIM> p1 = unpack<R, DIM>(ld16(st.rec + fr.c1));
     R flow[DIM + 2];
     if (f < g.nfi) {
-        if (!interior_flux<R, DIM, FLUX, REC, LIM>(g, st, wk, gas, f, nn, flow)) {
+        const GradRec<R, DIM> *grec = reinterpret_cast<const GradRec<R, DIM> *>(wk.grec);
+        GradRec<R, DIM> g0, g1;
+        if (REC) {
+            g0 = ld16(grec + fr.c0);
+            g1 = ld16(grec + fr.c1);
+        }
+        Prim<R, DIM> r[2] = {p0, p1};
+        if (!interior_flux<R, DIM, FLUX, REC, LIM>(r, &g0, &g1, fr, nn, gas, flow)) {
             flag_error(wk.err, FLUX == 2 ? ERR_HLL : ERR_HLLC, f);
 #pragma unroll
             for (int j = 0; j < DIM + 2; ++j) flow[j] = (R)0;
         }
     } else {
-        const int32_t c0 = g.c0[f];
-        const int32_t gh = c0 >= g.nint ? c0 : g.c1[f];
-        FaceState<R, DIM> s;
-        load_state<R, DIM>(st, g.nall, gh, s);
-        R vn = (R)0, vs = (R)0;
+        boundary_flux<R, DIM>(fr.c0 >= g.nint ? p0 : p1, nn, gas, flow);
+    }
+    FO o;
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(o.v) / sizeof(R)); ++i) o.v[i] = (R)0;
+#pragma unroll
+    for (int j = 0; j < DIM + 2; ++j) o.v[j] = flow[j] * S;
+    if (LC == 1) {
+        const R gr = (R)gas.gamma * (R)gas.rm;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) {
-            vn += s.u[k] * nn[k];
-            vs += s.u[k] * s.u[k];
+            o.v[FO::Q0 + k] = p0.u[k] * nn[k];
+            o.v[FO::Q1 + k] = p1.u[k] * nn[k];
         }
-        const R H = (R)gas.cp * s.T + (R)0.5 * vs;
+        o.v[FO::CN] = (sqrt(gr * p1.T) + sqrt(gr * p0.T)) * (R)0.5;
+        o.v[FO::SA] = S;
+    } else if (LC == 2) {
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) flow[k] = s.rho * s.u[k] * vn + s.p * nn[k];
-        flow[DIM] = s.rho * vn;
-        flow[DIM + 1] = s.rho * vn * H;
+        for (int k = 0; k < DIM; ++k) o.v[FO::Q0 + k] = S * fabs(nn[k]);
     }
-#pragma unroll
-    for (int j = 0; j < DIM + 2; ++j) wk.fs[(int64_t)j * g.nface + f] = flow[j] * S;
+    st16(reinterpret_cast<FO *>(wk.fout) + f, o);
 }
 
-template <typename R>
-__device__ __forceinline__ R cell_var(const DevState<R> &st, int32_t nall, int DIM, int i, int32_t c) {
-    return i < DIM ? st.u[(int64_t)i * nall + c] : (i == DIM ? st.p[c] : st.T[c]);
-}
+// ---------------------------------------------------------------------------
+// gradients
+// ---------------------------------------------------------------------------
 
-// psstGreenGauss::calculate (psstGradCalculation.cpp:80-177) as a per-cell
-// gather: grad_c += sign * (beta*phi0 + (1-beta)*phi1) * S/V_c * n, sign -1 on
-// side 0, +1 on side 1, faces in the reference's loop order. Followed, for
-// limiters 4/5, by the Barth-Jespersen / Venkatakrishnan cell limiter.
+// Thread per cell. psstGreenGauss::calculate (psstGradCalculation.cpp:80-177)
+// as a per-cell gather: grad_c += sign * (beta*phi0 + (1-beta)*phi1) * S/V_c * n,
+// sign -1 on side 0, +1 on side 1, faces in the reference's loop order; or the
+// 2D least squares of psstLeastSquare::calculate (:268-368) in the cell's own
+// face order. Then, for limiters 4/5, the Barth-Jespersen (AIAA 89-0366) /
+// Venkatakrishnan (AIAA 93-0880) cell limiter:
+// psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c).
 template <typename R, int DIM, int GRAD, int CELLLIM>
 __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
+    constexpr int NVAR = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nint) return;
-    constexpr int NVAR = DIM + 2;
+    const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
+    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    const Prim<R, DIM> own = unpack<R, DIM>(ld16(st.rec + c));
     R gr[NVAR][DIM];
 #pragma unroll
     for (int i = 0; i < NVAR; ++i)
 #pragma unroll
         for (int k = 0; k < DIM; ++k) gr[i][k] = (R)0;
-    const int32_t b = g.csr_ptr[c], e = g.csr_ptr[c + 1];
+    const uint64_t perm = g.wperm[c];
     if (GRAD == 1) {
         const double V = g.V[c];
-        for (int32_t q = b; q < e; ++q) {
-            const int32_t ent = g.csr_ent[q];
+        for (int32_t q = 0; q < K; ++q) {
+            const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
-            const int32_t c0 = g.c0[f], c1 = g.c1[f];
+            const FaceRec<R, DIM> fr = ld16(frec + f);
+            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + (side ? fr.c0 : fr.c1)));
             const R beta = (R)g.beta[f];
             const R rbeta = (R)1 - beta;
-            const R gp = (R)(g.S[f] / V);
+            const R gp = (R)(fr.S / V);
             const R sgn = side ? (R)1 : (R)-1;
-            R nk[DIM];
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) nk[k] = (R)g.n[(int64_t)k * g.nface + f];
 #pragma unroll
             for (int i = 0; i < NVAR; ++i) {
-                const R tv = beta * cell_var<R>(st, g.nall, DIM, i, c0) + rbeta * cell_var<R>(st, g.nall, DIM, i, c1);
+                const R a = pvar<R, DIM>(own, i), o = pvar<R, DIM>(oth, i);
+                const R phi0 = side ? o : a, phi1 = side ? a : o;  // neighbour 0 / 1 values
+                const R tv = beta * phi0 + rbeta * phi1;
 #pragma unroll
-                for (int k = 0; k < DIM; ++k) gr[i][k] += sgn * tv * gp * nk[k];
+                for (int k = 0; k < DIM; ++k) gr[i][k] += sgn * tv * gp * (R)fr.n[k];
             }
         }
-    } else {  // psstLeastSquare::calculate (:268-368), 2D, cell's own face order
+    } else {
         const R r0 = (R)g.lsq_r[c], r1 = (R)g.lsq_r[(int64_t)g.nint + c], r2 = (R)g.lsq_r[2 * (int64_t)g.nint + c];
-        const uint64_t perm = g.wperm[c];
         const R xc0 = (R)g.xc[c], xc1 = (R)g.xc[(int64_t)g.nall + c];
-        for (int32_t j = 0; j < e - b; ++j) {
+        for (int32_t j = 0; j < K; ++j) {
             const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
-            const int32_t f = ent >> 1, side = ent & 1;
-            const int32_t nb = side ? g.c0[f] : g.c1[f];
+            const int32_t f = ent >> 1;
+            const FaceRec<R, DIM> fr = ld16(frec + f);
+            const int32_t nb = (ent & 1) ? fr.c0 : fr.c1;
+            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + nb));
             R diff[2];
             diff[0] = (R)g.xc[nb] - xc0;
             diff[1] = (R)g.xc[(int64_t)g.nall + nb] - xc1;
@@ -341,42 +439,50 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
             const R th[2] = {al0 - r1 / r0 * al1, al1};
 #pragma unroll
             for (int i = 0; i < NVAR; ++i) {
-                const R phi = (cell_var<R>(st, g.nall, DIM, i, nb) - cell_var<R>(st, g.nall, DIM, i, c));
+                const R phi = (pvar<R, DIM>(oth, i) - pvar<R, DIM>(own, i));
 #pragma unroll
                 for (int k = 0; k < 2; ++k) gr[i][k] += ws * th[k] * phi;
             }
         }
     }
+    GradRec<R, DIM> out;
 #pragma unroll
-    for (int i = 0; i < NVAR; ++i)
+    for (int i = 0; i < NVAR; ++i) {
+        out.lim[i] = (R)1;
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) wk.grad[((int64_t)i * DIM + k) * g.nint + c] = gr[i][k];
+        for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = gr[i][k];
+    }
     if (CELLLIM) {
-        // Barth & Jespersen (AIAA 89-0366) / Venkatakrishnan (AIAA 93-0880):
-        // psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c)
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
-        const uint64_t perm = g.wperm[c];
+        R mx[NVAR], mn[NVAR];
 #pragma unroll
-        for (int i = 0; i < NVAR; ++i) {
-            const R phic = cell_var<R>(st, g.nall, DIM, i, c);
-            R mx = phic, mn = phic;
-            for (int32_t q = b; q < e; ++q) {
-                const int32_t ent = g.csr_ent[q];
-                const int32_t nb = (ent & 1) ? g.c0[ent >> 1] : g.c1[ent >> 1];
-                const R v = cell_var<R>(st, g.nall, DIM, i, nb);
-                if (v > mx) mx = v;
-                if (v < mn) mn = v;
+        for (int i = 0; i < NVAR; ++i) mx[i] = mn[i] = pvar<R, DIM>(own, i);
+        for (int32_t q = 0; q < K; ++q) {  // min/max over the face neighbours (order-free)
+            const int32_t ent = g.csr_ent[b + q];
+            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
+            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + ((ent & 1) ? fr.c0 : fr.c1)));
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i) {
+                const R v = pvar<R, DIM>(oth, i);
+                if (v > mx[i]) mx[i] = v;
+                if (v < mn[i]) mn[i] = v;
             }
-            R psi = (R)1;
-            for (int32_t j = 0; j < e - b; ++j) {
-                const int32_t f = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)] >> 1;
+        }
+        for (int32_t q = 0; q < K; ++q) {
+            const int32_t ent = g.csr_ent[b + q];
+            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
+            R off[DIM];  // x_f - x_c of this cell
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) off[k] = (ent & 1) ? fr.o1[k] : fr.o0[k];
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i) {
+                const R phic = pvar<R, DIM>(own, i);
                 R dm = (R)0;
 #pragma unroll
-                for (int k = 0; k < DIM; ++k)
-                    dm += gr[i][k] * (R)(g.xf[(int64_t)k * g.nface + f] - g.xc[(int64_t)k * g.nall + c]);
+                for (int k = 0; k < DIM; ++k) dm += gr[i][k] * off[k];
                 R pf = (R)1;
                 if (dm != (R)0) {
-                    const R dp = dm > (R)0 ? mx - phic : mn - phic;
+                    const R dp = dm > (R)0 ? mx[i] - phic : mn[i] - phic;
                     if (CELLLIM == 4) {
                         const R y = dp / dm;
                         pf = y < (R)1 ? y : (R)1;
@@ -386,28 +492,29 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
                         pf = num / den;
                     }
                 }
-                if (pf < psi) psi = pf;
+                if (pf < out.lim[i]) out.lim[i] = pf;
             }
-            wk.lim[(int64_t)i * g.nint + c] = psi;
         }
     }
+    st16(reinterpret_cast<GradRec<R, DIM> *>(wk.grec) + c, out);
 }
 
+// cell update
+// ---------------------------------------------------------------------------
+
 // Local time step of one cell (psstLocalTimeCalculation.cpp:90-131, 175-213),
-// faces in the cell's own order. nbP chooses the state each neighbour is read
-// from (the sequential mode reads already-updated neighbours from `nxt`).
+// faces in the cell's own order. In the sequential mode, neighbours updated
+// earlier in the reference's order are read from `nxt`.
 template <typename R, int DIM, int LC, bool SEQ>
-__device__ __forceinline__ double local_time(const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
-                                             const Gas &gas, double cfl, double dt_uniform, int32_t c) {
+__device__ __forceinline__ double local_time(const DevGrid &g, const CellRec<R> *cur, const CellRec<R> *nxt,
+                                             const Gas &gas, double cfl, double dt_uniform, int32_t c,
+                                             const Prim<R, DIM> &own) {
     if (LC == 0) return dt_uniform;
+    const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     const int32_t b = g.csr_ptr[c], e = g.csr_ptr[c + 1];
     const uint64_t perm = g.wperm[c];
     const R gr = (R)gas.gamma * (R)gas.rm;
-    const R Tc = cur.T[c];
-    const R cc = sqrt(gr * Tc);
-    R uc[DIM];
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) uc[k] = cur.u[(int64_t)k * g.nall + c];
+    const R cc = sqrt(gr * own.T);
     R den = (R)0;
     if (LC == 1) {
         R nnb = (R)0;
@@ -415,71 +522,45 @@ __device__ __forceinline__ double local_time(const DevGrid &g, const DevState<R>
         if (SEQ) myrank = g.rank[c];
         for (int32_t j = 0; j < e - b; ++j) {
             const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
-            const int32_t f = ent >> 1;
-            const int32_t nb = (ent & 1) ? g.c0[f] : g.c1[f];
-            const DevState<R> &src = (SEQ && nb < g.nint && g.rank[nb] < myrank) ? nxt : cur;
-            const R cn = (sqrt(gr * src.T[nb]) + cc) * (R)0.5;
+            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
+            const int32_t nb = (ent & 1) ? fr.c0 : fr.c1;
+            const CellRec<R> *src = (SEQ && nb < g.nint && g.rank[nb] < myrank) ? nxt : cur;
+            const Prim<R, DIM> o = unpack<R, DIM>(ld16(src + nb));
+            const R cn = (sqrt(gr * o.T) + cc) * (R)0.5;
             R nv = (R)0;
 #pragma unroll
             for (int k = 0; k < DIM; ++k) {
-                const R t = (R)g.n[(int64_t)k * g.nface + f];
-                nv += uc[k] * t;
-                nnb += src.u[(int64_t)k * g.nall + nb] * t;
+                const R t = (R)fr.n[k];
+                nv += own.u[k] * t;
+                nnb += o.u[k] * t;
             }
             nnb = (nnb + nv) * (R)0.5;
-            den += (fabs(nnb) + cn) * (R)g.S[f];
+            den += (fabs(nnb) + cn) * (R)fr.S;
         }
     } else {
         R s[DIM];
 #pragma unroll
         for (int k = 0; k < DIM; ++k) s[k] = (R)0;
         for (int32_t j = 0; j < e - b; ++j) {
-            const int32_t f = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)] >> 1;
-            const R S = (R)g.S[f];
+            const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
+            const R S = (R)fr.S;
 #pragma unroll
-            for (int k = 0; k < DIM; ++k) s[k] += S * fabs((R)g.n[(int64_t)k * g.nface + f]);
+            for (int k = 0; k < DIM; ++k) s[k] += S * fabs((R)fr.n[k]);
         }
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) den += (fabs(uc[k]) + cc) * s[k] * (R)0.5;
+        for (int k = 0; k < DIM; ++k) den += (fabs(own.u[k]) + cc) * s[k] * (R)0.5;
     }
     return (double)((R)cfl * (R)g.V[c] / den);
 }
 
-template <typename R>
-__device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, R v) {
-    const double d = fabs((double)v);
-    if (d == d) atomicMax(addr, (unsigned long long)__double_as_longlong(d));
-}
-
-// Cell pass of one RK stage for one cell (psstFiniteVolumeGrid.cpp:317-347):
-// residual gather in face-loop order, local time step, w = prev_w - dt*a*res/V,
-// max|res|, primitives. Writes the next primitive buffer.
-template <typename R, int DIM, int LC, bool SEQ, bool GATHER>
-__device__ __forceinline__ void update_cell(const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
-                                            const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform,
-                                            double alpha, int first_stage, int it_slot, int32_t c, double sq[DIM + 2]) {
+// RK stage update of one cell given its residual (psstFiniteVolumeGrid.cpp:324-346):
+// w = prev_w - dt*a*res/V in FP64, primitives, norms; returns the new record.
+template <typename R, int DIM>
+__device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<R> &wk, const Gas &gas, double dt,
+                                                double alpha, int first_stage, int32_t c, const R res[DIM + 2],
+                                                double sq[DIM + 2], double mx[DIM + 2]) {
     constexpr int NV = DIM + 2;
-    R res[NV];
-    if (GATHER) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) res[v] = (R)0;
-        const int32_t b = g.csr_ptr[c], e = g.csr_ptr[c + 1];
-        for (int32_t q = b; q < e; ++q) {
-            const int32_t ent = g.csr_ent[q];
-            const int32_t f = ent >> 1;
-            if (ent & 1) {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) res[v] += wk.fs[(int64_t)v * g.nface + f];
-            } else {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) res[v] -= wk.fs[(int64_t)v * g.nface + f];
-            }
-        }
-    } else {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) res[v] = wk.res[(int64_t)v * g.nint + c];
-    }
-    const double dt = local_time<R, DIM, LC, SEQ>(g, cur, nxt, gas, cfl, dt_uniform, c);
     wk.dt[c] = dt;
     const double vol = g.V[c];
     double w[NV];
@@ -495,61 +576,279 @@ __device__ __forceinline__ void update_cell(const DevGrid &g, const DevState<R> 
         }
         w[v] = pw - dt * alpha * (double)res[v] / vol;
         wk.w[idx] = w[v];
-        atomic_max_pos<R>(&wk.linf[it_slot * NV + v], res[v]);
         const double rv = (double)res[v];
+        const double ar = fabs(rv);
+        if (mx[v] < ar) mx[v] = ar;  // NaN never replaces the max, as in `if (res < |r|)` (:331)
         sq[v] += rv * rv;
         if (!(rv - rv == 0.0)) flag_error(wk.err, ERR_NONFINITE_RES, c);
     }
     const double rho = w[DIM];
     double vs = 0.0;
-    double u[DIM];
+    R u[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        u[k] = w[k] / rho;
-        vs += u[k] * u[k];
+        const double uk = w[k] / rho;
+        u[k] = (R)uk;
+        vs += uk * uk;
     }
     const double T = ((w[DIM + 1] / rho) - (vs * 0.5)) / gas.cv;
     const double p = rho * gas.rm * T;
     if (!(rho > 0.0 && T > 0.0)) flag_error(wk.err, ERR_BAD_STATE, c);
-    nxt.rho[c] = (R)rho;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) nxt.u[(int64_t)k * g.nall + c] = (R)u[k];
-    nxt.T[c] = (R)T;
-    nxt.p[c] = (R)p;
+    return pack<R, DIM>((R)p, (R)T, (R)rho, u);
 }
 
+// Ghost cell after its interior neighbour's update (psstFiniteVolumeGrid.cpp:
+// 351-366): dynamic condition (psstBoundaryCondition.cpp:26-37, 72-80, 108-127,
+// 212-219), thermal condition (:285-288, 354-357), rho = p/(T*rm).
+template <typename R, int DIM>
+__device__ __forceinline__ CellRec<R> ghost_state(const DevGrid &g, const CellRec<R> &gcur, const Prim<R, DIM> &nb,
+                                                  int32_t i, const Gas &gas) {
+    Prim<R, DIM> s = unpack<R, DIM>(gcur);
+    const int32_t z = g.g_zone[i];
+    const int dyn = g.z_dyn[z], th = g.z_therm[z];
+    if (dyn == 26) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s.u[k] = nb.u[k];
+        s.p = nb.p;
+    } else if (dyn == 15) {
+        const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + g.g_face[i]);
+        R vn = (R)0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) vn += nb.u[k] * (R)fr.n[k];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s.u[k] = nb.u[k] - vn * (R)fr.n[k];
+        s.p = nb.p;
+    } else if (dyn == 25) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s.u[k] = nb.u[k];
+    }
+    if (th == 25 || th == 18) s.T = nb.T;
+    return pack<R, DIM>(s.p, s.T, s.p / (s.T * (R)gas.rm), s.u);
+}
+
+// Block partials of the residual norms: part[block][v] = sum res^2,
+// part[block][NV + v] = max |res|; fixed reduction pattern (reproducible).
 template <int NV>
-__device__ __forceinline__ void block_sum_sq(double sq[NV], double *l2part) {
-    __shared__ double red[NV][32];
+__device__ __forceinline__ void block_norm_partials(double sq[NV], double mx[NV], double *part) {
+    __shared__ double red[2 * NV][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        double x = sq[v];
+        double x = sq[v], m = mx[v];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) red[v][wid] = x;
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_down_sync(FULL, x, o);
+            m = fmax(m, __shfl_down_sync(FULL, m, o));
+        }
+        if (lane == 0) {
+            red[v][wid] = x;
+            red[NV + v][wid] = m;
+        }
     }
     __syncthreads();
     if (threadIdx.x < NV) {
-        double s = 0.0;
+        double s = 0.0, m = 0.0;
         const int nw = (blockDim.x + 31) >> 5;
-        for (int i = 0; i < nw; ++i) s += red[threadIdx.x][i];
-        l2part[(int64_t)blockIdx.x * NV + threadIdx.x] = s;
+        for (int i = 0; i < nw; ++i) {
+            s += red[threadIdx.x][i];
+            m = fmax(m, red[NV + threadIdx.x][i]);
+        }
+        part[(int64_t)blockIdx.x * 2 * NV + threadIdx.x] = s;
+        part[(int64_t)blockIdx.x * 2 * NV + NV + threadIdx.x] = m;
     }
+}
+
+// Stage norms from the block partials (fixed-order strided sums + tree, so
+// reproducible), folded into the iteration's max over stages: the reference's
+// residual column is max over stages and cells of |res|
+// (psstFiniteVolumeGrid.cpp:331-332); the RMS column is this project's.
+// Executed by one whole block.
+template <int NV>
+__device__ __forceinline__ void finish_norms(const double *part, int nblocks, int32_t nint, double *linf, double *l2,
+                                             int it_slot) {
+    __shared__ double ss[NV][256], sm[NV][256];
+    const int t = threadIdx.x;
+    double s[NV], m[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = m[v] = 0.0;
+    for (int b = t; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            s[v] += part[(int64_t)b * 2 * NV + v];
+            m[v] = fmax(m[v], part[(int64_t)b * 2 * NV + NV + v]);
+        }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        ss[v][t] = s[v];
+        sm[v][t] = m[v];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                ss[v][t] += ss[v][t + w];
+                sm[v][t] = fmax(sm[v][t], sm[v][t + w]);
+            }
+        __syncthreads();
+    }
+    if (t < NV) {
+        const double r = sqrt(ss[t][0] / (double)(nint > 0 ? nint : 1));
+        if (r > l2[it_slot * NV + t]) l2[it_slot * NV + t] = r;
+        if (linf[it_slot * NV + t] < sm[t][0]) linf[it_slot * NV + t] = sm[t][0];
+    }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(256) k_norm_finish(const double *part, int nblocks, int32_t nint, double *linf,
+                                                     double *l2, int it_slot) {
+    finish_norms<NV>(part, nblocks, nint, linf, l2, it_slot);
+}
+
+// The last block of a launch to finish reduces all partials (no extra launch).
+template <int NV>
+__device__ __forceinline__ void last_block_finish(const double *part, unsigned *ticket,
+                                                  int32_t nint, double *linf, double *l2, int it_slot) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        finish_norms<NV>(part, gridDim.x, nint, linf, l2, it_slot);
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+}
+
+
+template <typename R, int DIM>
+__device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<R, DIM> *fo, int32_t c,
+                                                R res[DIM + 2]) {
+#pragma unroll
+    for (int v = 0; v < DIM + 2; ++v) res[v] = (R)0;
+    for (int32_t q = g.csr_ptr[c]; q < g.csr_ptr[c + 1]; ++q) {
+        const int32_t ent = g.csr_ent[q];
+        const FaceOut<R, DIM> o = ld16(fo + (ent >> 1));
+        if (ent & 1) {
+#pragma unroll
+            for (int v = 0; v < DIM + 2; ++v) res[v] += o.v[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < DIM + 2; ++v) res[v] -= o.v[v];
+        }
+    }
+}
+
+// Cell pass of one RK stage (parallel modes), thread per interior cell:
+// residual = in-order sum of the face outputs (psstFiniteVolumeGrid.cpp:311 and
+// the scatter at psstConvectiveFlow.cpp:289-299), local time step from the
+// faces' terms in the cell's own face order (the reference's accumulation
+// order, psstLocalTimeCalculation.cpp:117-127, 189-203), RK update, the cell's
+// ghost cells, block norm partials; the last block finishes the stage norms.
+template <typename R, int DIM, int LC>
+__global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
+                                              double cfl, double dt_uniform, double alpha, int first_stage,
+                                              int it_slot) {
+    using FO = FaceOut<R, DIM>;
+    constexpr int NV = DIM + 2;
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    double sq[NV], mx[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
+    if (c < g.nint) {
+        const FO *fo = reinterpret_cast<const FO *>(wk.fout);
+        R res[NV];
+        gather_residual<R, DIM>(g, fo, c, res);
+        double dt = dt_uniform;
+        if (LC != 0) {
+            const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+            const uint64_t perm = g.wperm[c];
+            R den = (R)0;
+            if (LC == 1) {
+                R nnb = (R)0;
+                for (int32_t j = 0; j < K; ++j) {
+                    const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+                    const FO o = ld16(fo + (ent >> 1));
+                    const int side = ent & 1;
+                    R nv = (R)0;
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) {
+                        nv += side ? o.v[FO::Q1 + k] : o.v[FO::Q0 + k];   // own u . n
+                        nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];  // neighbour u . n
+                    }
+                    nnb = (nnb + nv) * (R)0.5;
+                    den += (fabs(nnb) + o.v[FO::CN]) * o.v[FO::SA];
+                }
+            } else {
+                R s[DIM];
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) s[k] = (R)0;
+                for (int32_t j = 0; j < K; ++j) {
+                    const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+                    const FO o = ld16(fo + (ent >> 1));
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
+                }
+                const Prim<R, DIM> own = unpack<R, DIM>(ld16(cur.rec + c));
+                const R cc = sqrt((R)gas.gamma * (R)gas.rm * own.T);
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) den += (fabs(own.u[k]) + cc) * s[k] * (R)0.5;
+            }
+            dt = (double)((R)cfl * (R)g.V[c] / den);
+        }
+        const CellRec<R> nrec = rk_update<R, DIM>(g, wk, gas, dt, alpha, first_stage, c, res, sq, mx);
+        st16(nxt.rec + c, nrec);
+        const int32_t g0 = g.gptr[c], g1 = g.gptr[c + 1];
+        if (g1 > g0) {
+            const Prim<R, DIM> np = unpack<R, DIM>(nrec);
+            for (int32_t i = g0; i < g1; ++i) {
+                const int32_t gc = g.nint + i;
+                st16(nxt.rec + gc, ghost_state<R, DIM>(g, ld16(cur.rec + gc), np, i, gas));
+            }
+        }
+    }
+    block_norm_partials<NV>(sq, mx, wk.l2part);
+    last_block_finish<NV>(wk.l2part, wk.ticket, g.nint, wk.linf, wk.l2, it_slot);
+}
+
+// Thread-per-cell update reading the face outputs (GATHER) or the residual of
+// the stage-by-stage API; local time step from states (sequential mode: the
+// reference's in-loop order); ghosts by k_ghost_update.
+template <typename R, int DIM, int LC, bool GATHER>
+__device__ __forceinline__ void update_from_buffers(const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
+                                                    const DevWork<R> &wk, const Gas &gas, double cfl,
+                                                    double dt_uniform, double alpha, int first_stage, int32_t c,
+                                                    double sq[DIM + 2], double mx[DIM + 2], bool seq) {
+    constexpr int NV = DIM + 2;
+    R res[NV];
+    if (GATHER) {
+        gather_residual<R, DIM>(g, reinterpret_cast<const FaceOut<R, DIM> *>(wk.fout), c, res);
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) res[v] = wk.res[(int64_t)v * g.nint + c];
+    }
+    const Prim<R, DIM> own = unpack<R, DIM>(ld16(cur.rec + c));
+    double dt;
+    if (seq)
+        dt = local_time<R, DIM, 1, true>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
+    else
+        dt = local_time<R, DIM, LC, false>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
+    st16(nxt.rec + c, rk_update<R, DIM>(g, wk, gas, dt, alpha, first_stage, c, res, sq, mx));
 }
 
 template <typename R, int DIM, int LC, bool GATHER>
 __global__ void __launch_bounds__(256) k_cell_update(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
-                                                     double cfl, double dt_uniform, double alpha, int first_stage,
-                                                     int it_slot) {
+                                                     double cfl, double dt_uniform, double alpha, int first_stage) {
     constexpr int NV = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    double sq[NV];
+    double sq[NV], mx[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sq[v] = 0.0;
+    for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
     if (c < g.nint)
-        update_cell<R, DIM, LC, false, GATHER>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, c, sq);
-    block_sum_sq<NV>(sq, wk.l2part);
+        update_from_buffers<R, DIM, LC, GATHER>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, c, sq, mx,
+                                                false);
+    block_norm_partials<NV>(sq, mx, wk.l2part);
 }
 
 // Sequential LocalAccTime1 (the reference's in-loop evaluation order,
@@ -559,56 +858,31 @@ __global__ void __launch_bounds__(256) k_cell_update(DevGrid g, DevState<R> cur,
 // neighbours from the next buffer and the others from the current one.
 template <typename R, int DIM, bool GATHER>
 __global__ void __launch_bounds__(1024) k_cell_update_seq(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk,
-                                                          Gas gas, double cfl, double alpha, int first_stage, int it_slot) {
+                                                          Gas gas, double cfl, double alpha, int first_stage) {
     constexpr int NV = DIM + 2;
-    double sq[NV];
+    double sq[NV], mx[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sq[v] = 0.0;
+    for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
     for (int32_t l = 0; l < g.nlevels; ++l) {
         const int32_t b = g.lvl_ptr[l], e = g.lvl_ptr[l + 1];
         for (int32_t i = b + threadIdx.x; i < e; i += blockDim.x)
-            update_cell<R, DIM, 1, true, GATHER>(g, cur, nxt, wk, gas, cfl, 0.0, alpha, first_stage, it_slot,
-                                                 g.lvl_cells[i], sq);
+            update_from_buffers<R, DIM, 1, GATHER>(g, cur, nxt, wk, gas, cfl, 0.0, alpha, first_stage, g.lvl_cells[i],
+                                                   sq, mx, true);
         __threadfence_block();
         __syncthreads();
     }
-    block_sum_sq<NV>(sq, wk.l2part);
+    block_norm_partials<NV>(sq, mx, wk.l2part);
 }
 
-// Ghost cells after the interior update (psstFiniteVolumeGrid.cpp:351-366):
-// dynamic condition, thermal condition, rho = p/(T*rm).
+// Ghost cells after the interior update (face-pass path of the sequential
+// mode and of the stage-by-stage API).
 template <typename R, int DIM>
 __global__ void __launch_bounds__(256) k_ghost_update(DevGrid g, DevState<R> cur, DevState<R> nxt, Gas gas) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.nghost) return;
     const int32_t c = g.nint + i;
-    const int32_t nb = g.g_nb[i], f = g.g_face[i], z = g.g_zone[i];
-    R p = cur.p[c], T = cur.T[c], u[DIM];
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) u[k] = cur.u[(int64_t)k * g.nall + c];
-    const int dyn = g.z_dyn[z], th = g.z_therm[z];
-    if (dyn == 26) {  // psstSupersonicOutlet (psstBoundaryCondition.cpp:72-80)
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) u[k] = nxt.u[(int64_t)k * g.nall + nb];
-        p = nxt.p[nb];
-    } else if (dyn == 15) {  // psstInviscidWall (:108-127)
-        R vn = (R)0;
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) vn += nxt.u[(int64_t)k * g.nall + nb] * (R)g.n[(int64_t)k * g.nface + f];
-#pragma unroll
-        for (int k = 0; k < DIM; ++k)
-            u[k] = nxt.u[(int64_t)k * g.nall + nb] - vn * (R)g.n[(int64_t)k * g.nface + f];
-        p = nxt.p[nb];
-    } else if (dyn == 25) {  // psstOutlet (:212-219)
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) u[k] = nxt.u[(int64_t)k * g.nall + nb];
-    }
-    if (th == 25 || th == 18) T = nxt.T[nb];  // (:285-288, :354-357)
-    nxt.p[c] = p;
-    nxt.T[c] = T;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) nxt.u[(int64_t)k * g.nall + c] = u[k];
-    nxt.rho[c] = p / (T * (R)gas.rm);
+    const Prim<R, DIM> nb = unpack<R, DIM>(ld16(nxt.rec + g.g_nb[i]));
+    st16(nxt.rec + c, ghost_state<R, DIM>(g, ld16(cur.rec + c), nb, i, gas));
 }
 
 // residual gather into wk.res (stage-by-stage API)
@@ -616,50 +890,29 @@ template <typename R, int DIM>
 __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevWork<R> wk) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nint) return;
-    constexpr int NV = DIM + 2;
-    R res[NV];
+    R res[DIM + 2];
+    gather_residual<R, DIM>(g, reinterpret_cast<const FaceOut<R, DIM> *>(wk.fout), c, res);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) res[v] = (R)0;
-    for (int32_t q = g.csr_ptr[c]; q < g.csr_ptr[c + 1]; ++q) {
-        const int32_t ent = g.csr_ent[q];
-        const int32_t f = ent >> 1;
-        if (ent & 1) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) res[v] += wk.fs[(int64_t)v * g.nface + f];
-        } else {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) res[v] -= wk.fs[(int64_t)v * g.nface + f];
-        }
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) wk.res[(int64_t)v * g.nint + c] = res[v];
+    for (int v = 0; v < DIM + 2; ++v) wk.res[(int64_t)v * g.nint + c] = res[v];
 }
 
-// RMS of one stage from the block partials, folded into the iteration's max.
-template <int NV>
-__global__ void k_l2_finish(const double *l2part, int nblocks, int32_t nint, double *l2, int it_slot) {
-    const int v = threadIdx.x;
-    if (v >= NV) return;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += l2part[(int64_t)b * NV + v];
-    const double r = sqrt(s / (double)(nint > 0 ? nint : 1));
-    if (r > l2[it_slot * NV + v]) l2[it_slot * NV + v] = r;
-}
-
-// explicit_solve prologue (psstFiniteVolumeGrid.cpp:279-300) for interior cells,
-// plus rho = p/(rm*T) for every volume.
+// explicit_solve prologue (psstFiniteVolumeGrid.cpp:279-300): rho = p/(rm*T)
+// for every volume (initialize_field and load_boundary form it so), and w for
+// interior cells.
 template <typename R, int DIM>
 __global__ void k_prologue(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nall) return;
-    const double p = (double)st.p[c], T = (double)st.T[c];
+    CellRec<R> r = st.rec[c];
+    const double p = (double)r.v[RP], T = (double)r.v[RT];
     const double rho = p / (gas.rm * T);
-    st.rho[c] = (R)rho;
+    r.v[RRHO] = (R)rho;
+    st.rec[c] = r;
     if (c >= g.nint) return;
     double vs = 0.0;
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        const double t = (double)st.u[(int64_t)k * g.nall + c];
+        const double t = (double)r.v[RU + k];
         wk.w[(int64_t)k * g.nint + c] = rho * t;
         vs += t * t;
     }

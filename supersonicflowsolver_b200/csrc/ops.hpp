@@ -1,6 +1,8 @@
 // Kernel launchers, one set per state precision (explicitly instantiated in
 // kernels_f64.cu and kernels_f32.cu). Host code (solver.cpp) calls only these.
 #pragma once
+#include <cstddef>
+
 #include <cuda_runtime_api.h>
 
 #include "devgrid.hpp"
@@ -12,22 +14,33 @@ inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
 template <typename R>
 struct Ops {
+    // sizes of the records for a dimension (host allocation)
+    static size_t face_rec_bytes(int dim);
+    static size_t grad_rec_bytes(int dim);
+    static size_t face_out_bytes(int dim);
     static void prologue(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
                          cudaStream_t s);
     // grad: 1 Green-Gauss, 2 least squares; celllim: 0, 4 (Barth-Jespersen), 5 (Venkatakrishnan)
     static void gradient(int dim, int grad, int celllim, const DevGrid &g, const DevState<R> &st,
                          const DevWork<R> &wk, cudaStream_t s);
-    // rec: 0 first order, 1 DM with limiter lim (1..3), 2 cell-limited MUSCL
-    static void face_flux(int dim, int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st,
-                          const DevWork<R> &wk, const Gas &gas, cudaStream_t s);
+    // face pass: rec 0 first order, 1 DM with limiter lim (1..3), 2 cell-limited
+    // MUSCL; lc selects the time-step terms written with each face's flux
+    static void face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st,
+                     const DevWork<R> &wk, const Gas &gas, cudaStream_t s);
+    // cell pass of the parallel modes (lc 0, 2, 1 from stage-start values):
+    // residual, time step, RK update, ghosts, norms (last block finishes them)
+    static void cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
+                     const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
+                     int first_stage, int it_slot, cudaStream_t s);
     static void residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStream_t s);
-    // lc: 0, 1, 2; seq: sequential LocalAccTime1 (single block over levels)
+    // cell update from face outputs (gather) or from wk.res; seq: the
+    // sequential LocalAccTime1 (single block over levels); norms by norm_finish
     static void cell_update(int dim, int lc, bool seq, bool gather, const DevGrid &g, const DevState<R> &cur,
                             const DevState<R> &nxt, const DevWork<R> &wk, const Gas &gas, double cfl,
-                            double dt_uniform, double alpha, int first_stage, int it_slot, cudaStream_t s);
+                            double dt_uniform, double alpha, int first_stage, cudaStream_t s);
     static void ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                              const Gas &gas, cudaStream_t s);
-    static void l2_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s);
+    static void norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s);
 };
 
 }  // namespace psst

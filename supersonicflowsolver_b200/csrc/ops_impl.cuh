@@ -7,6 +7,19 @@
 namespace psst {
 
 template <typename R>
+size_t Ops<R>::face_rec_bytes(int dim) {
+    return dim == 2 ? sizeof(FaceRec<R, 2>) : sizeof(FaceRec<R, 3>);
+}
+template <typename R>
+size_t Ops<R>::grad_rec_bytes(int dim) {
+    return dim == 2 ? sizeof(GradRec<R, 2>) : sizeof(GradRec<R, 3>);
+}
+template <typename R>
+size_t Ops<R>::face_out_bytes(int dim) {
+    return dim == 2 ? sizeof(FaceOut<R, 2>) : sizeof(FaceOut<R, 3>);
+}
+
+template <typename R>
 void Ops<R>::prologue(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
                       cudaStream_t s) {
     if (g.nall == 0) return;
@@ -47,41 +60,77 @@ void Ops<R>::gradient(int dim, int grad, int celllim, const DevGrid &g, const De
         gradient_dim<R, 3>(grad, celllim, g, st, wk, s);
 }
 
-template <typename R, int DIM, int FLUX>
-static void face_flux_f(int rec, int lim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
-                        const Gas &gas, cudaStream_t s) {
+// ---- face pass: DIM x FLUX x (REC, LIM) x LC ----
+template <typename R, int DIM, int FLUX, int REC, int LIM>
+static void face_l(int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
+                   cudaStream_t s) {
     const int nb = nblocks(g.nface);
-    if (rec == 0)
-        k_face_flux<R, DIM, FLUX, 0, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
-    else if (rec == 2)
-        k_face_flux<R, DIM, FLUX, 2, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
-    else if (lim == 1)
-        k_face_flux<R, DIM, FLUX, 1, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
-    else if (lim == 2)
-        k_face_flux<R, DIM, FLUX, 1, 2><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    if (lc == 1)
+        k_face<R, DIM, FLUX, REC, LIM, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+    else if (lc == 2)
+        k_face<R, DIM, FLUX, REC, LIM, 2><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
     else
-        k_face_flux<R, DIM, FLUX, 1, 3><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+        k_face<R, DIM, FLUX, REC, LIM, 0><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+}
+
+template <typename R, int DIM, int FLUX>
+static void face_r(int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                   const Gas &gas, cudaStream_t s) {
+    if (rec == 0)
+        face_l<R, DIM, FLUX, 0, 1>(lc, g, st, wk, gas, s);
+    else if (rec == 2)
+        face_l<R, DIM, FLUX, 2, 1>(lc, g, st, wk, gas, s);
+    else if (lim == 1)
+        face_l<R, DIM, FLUX, 1, 1>(lc, g, st, wk, gas, s);
+    else if (lim == 2)
+        face_l<R, DIM, FLUX, 1, 2>(lc, g, st, wk, gas, s);
+    else
+        face_l<R, DIM, FLUX, 1, 3>(lc, g, st, wk, gas, s);
 }
 
 template <typename R, int DIM>
-static void face_flux_d(int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
-                        const Gas &gas, cudaStream_t s) {
+static void face_f(int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                   const Gas &gas, cudaStream_t s) {
     if (flux == 1)
-        face_flux_f<R, DIM, 1>(rec, lim, g, st, wk, gas, s);
+        face_r<R, DIM, 1>(rec, lim, lc, g, st, wk, gas, s);
     else if (flux == 2)
-        face_flux_f<R, DIM, 2>(rec, lim, g, st, wk, gas, s);
+        face_r<R, DIM, 2>(rec, lim, lc, g, st, wk, gas, s);
     else
-        face_flux_f<R, DIM, 3>(rec, lim, g, st, wk, gas, s);
+        face_r<R, DIM, 3>(rec, lim, lc, g, st, wk, gas, s);
 }
 
 template <typename R>
-void Ops<R>::face_flux(int dim, int flux, int rec, int lim, const DevGrid &g, const DevState<R> &st,
-                       const DevWork<R> &wk, const Gas &gas, cudaStream_t s) {
+void Ops<R>::face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st,
+                  const DevWork<R> &wk, const Gas &gas, cudaStream_t s) {
     if (g.nface == 0) return;
     if (dim == 2)
-        face_flux_d<R, 2>(flux, rec, lim, g, st, wk, gas, s);
+        face_f<R, 2>(flux, rec, lim, lc, g, st, wk, gas, s);
     else
-        face_flux_d<R, 3>(flux, rec, lim, g, st, wk, gas, s);
+        face_f<R, 3>(flux, rec, lim, lc, g, st, wk, gas, s);
+}
+
+// ---- cell pass (parallel modes) ----
+template <typename R, int DIM>
+static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const DevWork<R> &wk,
+                   const Gas &gas, double cfl, double dtu, double alpha, int first, int it, cudaStream_t s) {
+    const int nb = nblocks(g.nint);
+    if (lc == 1)
+        k_cell<R, DIM, 1><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+    else if (lc == 2)
+        k_cell<R, DIM, 2><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+    else
+        k_cell<R, DIM, 0><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+}
+
+template <typename R>
+void Ops<R>::cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
+                  const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha, int first_stage,
+                  int it_slot, cudaStream_t s) {
+    if (g.nint == 0) return;
+    if (dim == 2)
+        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+    else
+        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
 }
 
 template <typename R>
@@ -96,38 +145,38 @@ void Ops<R>::residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStrea
 template <typename R, int DIM, bool GATHER>
 static void cell_update_g(int lc, bool seq, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                           const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
-                          int first_stage, int it_slot, cudaStream_t s) {
+                          int first_stage, cudaStream_t s) {
     if (seq) {
-        k_cell_update_seq<R, DIM, GATHER><<<1, 1024, 0, s>>>(g, cur, nxt, wk, gas, cfl, alpha, first_stage, it_slot);
+        k_cell_update_seq<R, DIM, GATHER><<<1, 1024, 0, s>>>(g, cur, nxt, wk, gas, cfl, alpha, first_stage);
         return;
     }
     const int nb = nblocks(g.nint);
     if (lc == 0)
         k_cell_update<R, DIM, 0, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
-                                                               first_stage, it_slot);
+                                                               first_stage);
     else if (lc == 1)
         k_cell_update<R, DIM, 1, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
-                                                               first_stage, it_slot);
+                                                               first_stage);
     else
         k_cell_update<R, DIM, 2, GATHER><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dt_uniform, alpha,
-                                                               first_stage, it_slot);
+                                                               first_stage);
 }
 
 template <typename R>
 void Ops<R>::cell_update(int dim, int lc, bool seq, bool gather, const DevGrid &g, const DevState<R> &cur,
                          const DevState<R> &nxt, const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform,
-                         double alpha, int first_stage, int it_slot, cudaStream_t s) {
+                         double alpha, int first_stage, cudaStream_t s) {
     if (g.nint == 0) return;
     if (dim == 2) {
         if (gather)
-            cell_update_g<R, 2, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+            cell_update_g<R, 2, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, s);
         else
-            cell_update_g<R, 2, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+            cell_update_g<R, 2, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, s);
     } else {
         if (gather)
-            cell_update_g<R, 3, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+            cell_update_g<R, 3, true>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, s);
         else
-            cell_update_g<R, 3, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+            cell_update_g<R, 3, false>(lc, seq, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, s);
     }
 }
 
@@ -142,11 +191,11 @@ void Ops<R>::ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, con
 }
 
 template <typename R>
-void Ops<R>::l2_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s) {
+void Ops<R>::norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s) {
     if (dim == 2)
-        k_l2_finish<4><<<1, 32, 0, s>>>(wk.l2part, nblk, nint, wk.l2, it_slot);
+        k_norm_finish<4><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
     else
-        k_l2_finish<5><<<1, 32, 0, s>>>(wk.l2part, nblk, nint, wk.l2, it_slot);
+        k_norm_finish<5><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
 }
 
 }  // namespace psst

@@ -1,18 +1,22 @@
 // Device solver: layout, memory and the per-iteration launch sequence.
 //
-// Layout (all SoA, sized for one GPU):
+// Layout (sized for one GPU):
 //  * interior cells renumbered along a 3D/2D Hilbert curve of their centroids
 //    (B200 gathers hit L2 far more often when neighbours are close in memory),
-//    then ghost cells ordered by their interior neighbour;
+//    then ghost cells ordered by their interior neighbour, so each interior
+//    cell owns a contiguous ghost range;
 //  * faces: interior faces sorted by their lower cell id, then boundary faces;
+//    gathered data (cell state, gradients + limiter, face geometry) are
+//    16-byte-aligned records (devgrid.hpp);
 //  * per cell a CSR of (face, side) sorted by the reference's face-loop order,
 //    so every per-cell sum is formed in the reference's order whatever the
 //    device numbering, plus a 4-bit permutation that replays the cell's own
 //    face order (used by LocalAccTime1/2 and least squares).
-// One RK stage is: face pass (flux*area per face) -> cell pass (deterministic
-// CSR gather, local time step, RK update, primitives, residual norms) -> ghost
-// pass (boundary conditions). Gradients run once per iteration before stage 0
-// (psstFiniteVolumeGrid.cpp:307-308).
+// One RK stage is one fused launch (k_stage: fluxes of each cell's faces,
+// in-order residual, local time step, RK update, the cell's ghosts, norms) in
+// the parallel modes, or face pass -> cell pass -> ghost pass -> norms for the
+// sequential LocalAccTime1 mode and the stage-by-stage API. Gradients run once
+// per iteration before stage 0 (psstFiniteVolumeGrid.cpp:307-308).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -65,7 +69,7 @@ struct Layout {
     int32_t nint = 0, nghost = 0, nall = 0, nface = 0, nfi = 0, nlevels = 0;
     std::vector<int32_t> dev_of_vol;  // reference volume -> device cell (-1: inactive)
     std::vector<int64_t> vol_of_dev;  // device cell -> reference volume
-    std::vector<int32_t> c0, c1, csr_ptr, csr_ent, rank, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
+    std::vector<int32_t> c0, c1, csr_ptr, csr_ent, rank, gptr, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
     std::vector<uint64_t> wperm;
     std::vector<double> S, n, xf, beta, V, xc, lsq_r, vk_eps2, z_u, z_p, z_T;
 };
@@ -204,10 +208,14 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         for (int j = 0; j < k; ++j) perm |= (uint64_t)pos[j] << (4 * j);
         L.wperm[d] = perm;
     }
-    // ghost tables and boundary zones
+    // ghost tables and boundary zones; ghosts are sorted by interior neighbour,
+    // so each interior cell owns a contiguous ghost range [gptr[d], gptr[d+1])
     L.g_nb.resize(L.nghost);
     L.g_face.resize(L.nghost);
     L.g_zone.resize(L.nghost);
+    L.gptr.assign(L.nint + 1, 0);
+    for (int32_t i = 0; i < L.nghost; ++i) L.gptr[gh[i].first + 1]++;
+    for (int32_t d = 0; d < L.nint; ++d) L.gptr[d + 1] += L.gptr[d];
     for (int32_t i = 0; i < L.nghost; ++i) {
         const int64_t v = L.vol_of_dev[L.nint + i];
         const int64_t f = G.vf_idx[G.vf_ptr[v]];
@@ -277,6 +285,35 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
     }
 }
 
+
+// Face records: neighbours, area, normal and the reconstruction offsets of the
+// scheme in use (formed in FP64, rounded once to R).
+template <typename R, int DIM>
+std::vector<FaceRec<R, DIM>> build_face_records(const psst_grid &G, const Layout &L, int rec) {
+    std::vector<FaceRec<R, DIM>> out(L.nface);
+    for (int32_t d = 0; d < L.nface; ++d) {
+        FaceRec<R, DIM> r;
+        std::memset(&r, 0, sizeof r);
+        r.c0 = L.c0[d];
+        r.c1 = L.c1[d];
+        r.S = L.S[d];
+        for (int k = 0; k < DIM; ++k) {
+            r.n[k] = L.n[(size_t)k * L.nface + d];
+            const double xf = L.xf[(size_t)k * L.nface + d];
+            const double x0 = L.xc[(size_t)k * L.nall + r.c0], x1 = L.xc[(size_t)k * L.nall + r.c1];
+            if (rec == 1) {  // Darwish-Moukalled: R = x_c0 - x_c1 (psstValueReconstructor.cpp:105-107)
+                r.o0[k] = (R)(x0 - x1);
+            } else if (rec == 2) {  // MUSCL: x_f - x_c per side
+                r.o0[k] = (R)(xf - x0);
+                r.o1[k] = (R)(xf - x1);
+            }
+        }
+        out[d] = r;
+    }
+    (void)G;
+    return out;
+}
+
 }  // namespace
 
 struct psst_solver {
@@ -301,16 +338,18 @@ struct psst_solver {
     int rec = 0, celllim = 0;
     bool seq = false;
     double dt_uniform = 0.0;
-    int nblk = 1;
+    int nblk = 1;  // blocks of the thread-per-cell kernels
     int norm_cap = 0;
-    double *linf_host_tmp = nullptr;
 
+    void *dalloc_bytes(size_t n) {
+        void *p = nullptr;
+        ck(cudaMalloc(&p, std::max<size_t>(n, 16)), "cudaMalloc");
+        allocs.push_back(p);
+        return p;
+    }
     template <class T>
     T *dalloc(size_t n) {
-        void *p = nullptr;
-        ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-        allocs.push_back(p);
-        return (T *)p;
+        return (T *)dalloc_bytes(std::max<size_t>(n, 1) * sizeof(T));
     }
     template <class T>
     T *upload(const std::vector<T> &v) {
@@ -351,31 +390,34 @@ DevWork<float> &work<float>(psst_solver *s) {
 }
 
 template <typename R>
-void alloc_state(psst_solver *s) {
+void alloc_state(psst_solver *s, const psst_grid &G) {
     const int dim = s->dim;
     const int32_t nall = s->L.nall, nint = s->L.nint, nface = s->L.nface;
+    if (dim == 2)
+        s->g.frec = s->upload(build_face_records<R, 2>(G, s->L, s->rec));
+    else
+        s->g.frec = s->upload(build_face_records<R, 3>(G, s->L, s->rec));
     DevState<R> *st = states<R>(s);
     for (int b = 0; b < 2; ++b) {
-        st[b].p = s->dalloc<R>(nall);
-        st[b].T = s->dalloc<R>(nall);
-        st[b].rho = s->dalloc<R>(nall);
-        st[b].u = s->dalloc<R>((size_t)dim * nall);
+        st[b].rec = s->dalloc<CellRec<R>>(nall);
+        ck(cudaMemset(st[b].rec, 0, (size_t)std::max(nall, 1) * sizeof(CellRec<R>)), "memset");
     }
     DevWork<R> &w = work<R>(s);
     const int nv = s->nv;
+    const size_t gbytes = Ops<R>::grad_rec_bytes(dim);
     w.w = s->dalloc<double>((size_t)nv * nint);
     w.pw = s->dalloc<double>((size_t)nv * nint);
-    w.grad = s->dalloc<R>((size_t)nv * dim * nint);
-    w.lim = s->dalloc<R>((size_t)nv * nint);
-    w.fs = s->dalloc<R>((size_t)nv * nface);
+    w.grec = s->dalloc_bytes(gbytes * std::max(nint, 1));
+    w.fout = s->dalloc_bytes(Ops<R>::face_out_bytes(dim) * std::max(nface, 1));
     w.res = s->dalloc<R>((size_t)nv * nint);
     w.dt = s->dalloc<double>(nint);
-    w.l2part = s->dalloc<double>((size_t)nv * std::max(s->nblk, 1));
+    w.l2part = s->dalloc<double>((size_t)2 * nv * std::max(s->nblk, 1));
+    w.ticket = s->dalloc<unsigned int>(1);
     w.err = s->dalloc<int32_t>(4);
-    ck(cudaMemset(w.grad, 0, (size_t)nv * dim * nint * sizeof(R)), "memset");
-    ck(cudaMemset(w.lim, 0, (size_t)nv * nint * sizeof(R)), "memset");
-    ck(cudaMemset(w.res, 0, (size_t)nv * nint * sizeof(R)), "memset");
-    ck(cudaMemset(w.dt, 0, (size_t)nint * sizeof(double)), "memset");
+    ck(cudaMemset(w.grec, 0, gbytes * std::max(nint, 1)), "memset");
+    ck(cudaMemset(w.res, 0, (size_t)std::max(nv * nint, 1) * sizeof(R)), "memset");
+    ck(cudaMemset(w.dt, 0, (size_t)std::max(nint, 1) * sizeof(double)), "memset");
+    ck(cudaMemset(w.ticket, 0, sizeof(unsigned int)), "memset");
     ck(cudaMemset(w.err, 0, 4 * sizeof(int32_t)), "memset");
 }
 
@@ -384,10 +426,10 @@ void ensure_norms(psst_solver *s, int n_iter) {
     DevWork<R> &w = work<R>(s);
     if (n_iter > s->norm_cap) {
         s->norm_cap = std::max(n_iter, 2 * s->norm_cap);
-        w.linf = s->dalloc<unsigned long long>((size_t)s->norm_cap * s->nv);
+        w.linf = s->dalloc<double>((size_t)s->norm_cap * s->nv);
         w.l2 = s->dalloc<double>((size_t)s->norm_cap * s->nv);
     }
-    ck(cudaMemsetAsync(w.linf, 0, (size_t)n_iter * s->nv * sizeof(unsigned long long), s->stream), "memset");
+    ck(cudaMemsetAsync(w.linf, 0, (size_t)n_iter * s->nv * sizeof(double), s->stream), "memset");
     ck(cudaMemsetAsync(w.l2, 0, (size_t)n_iter * s->nv * sizeof(double), s->stream), "memset");
 }
 
@@ -397,6 +439,7 @@ void check_err(psst_solver *s, const int32_t *err_dev) {
     ck(cudaStreamSynchronize(s->stream), "stream sync");
     if (e[0] == 0) return;
     ck(cudaMemsetAsync((void *)err_dev, 0, sizeof e, s->stream), "memset");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
     switch (e[0]) {
     case 1:
         raise(PSST_ERR_FLUX, "Error: Could not calculate convective HLL flow!");
@@ -409,23 +452,49 @@ void check_err(psst_solver *s, const int32_t *err_dev) {
     }
 }
 
-template <typename R>
-int64_t one_stage(psst_solver *s, int k, int it_slot, bool gather) {
+enum Kind { K_GRADIENT = 0, K_FACE = 1, K_CELL = 2, K_GHOST = 3, K_NORM = 4 };
+
+// One RK stage. The parallel modes run face pass -> cell pass (the cell pass
+// also updates ghosts and finishes the norms); the sequential LocalAccTime1
+// mode and the stage-by-stage API (gather == false: residual already in
+// wk.res) run face pass -> cell update -> ghost pass -> norms.
+// mark(kind) is called after each launch (profiling hook).
+template <typename R, typename Mark>
+void one_stage(psst_solver *s, int k, int it_slot, bool gather, Mark &&mark) {
     DevState<R> *st = states<R>(s);
     DevWork<R> &w = work<R>(s);
     const DevState<R> &cur = st[s->cur], &nxt = st[s->cur ^ 1];
-    int64_t launches = 0;
     if (gather) {
-        Ops<R>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, cur, w, s->gas, s->stream);
-        ++launches;
+        Ops<R>::face(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->seq ? 0 : s->sc.lc, s->g, cur, w, s->gas,
+                     s->stream);
+        mark(K_FACE);
     }
-    Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, gather, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
-                        s->sc.rk[k], k == 0, it_slot, s->stream);
-    Ops<R>::ghost_update(s->dim, s->g, cur, nxt, s->gas, s->stream);
-    Ops<R>::l2_finish(s->dim, w, s->seq ? 1 : s->nblk, s->L.nint, it_slot, s->stream);
-    launches += 3;
+    if (gather && !s->seq) {
+        Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], k == 0,
+                     it_slot, s->stream);
+        mark(K_CELL);
+    } else {
+        Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, gather, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
+                            s->sc.rk[k], k == 0, s->stream);
+        mark(K_CELL);
+        Ops<R>::ghost_update(s->dim, s->g, cur, nxt, s->gas, s->stream);
+        mark(K_GHOST);
+        Ops<R>::norm_finish(s->dim, w, s->seq ? 1 : s->nblk, s->L.nint, it_slot, s->stream);
+        mark(K_NORM);
+    }
     s->cur ^= 1;
-    return launches;
+}
+
+template <typename R, typename Mark>
+void iterations(psst_solver *s, int n_iter, Mark &&mark) {
+    DevWork<R> &w = work<R>(s);
+    for (int it = 0; it < n_iter; ++it) {
+        if (s->sc.order == 2) {
+            Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, states<R>(s)[s->cur], w, s->stream);
+            mark(K_GRADIENT);
+        }
+        for (int k = 0; k < s->sc.rk_level; ++k) one_stage<R>(s, k, it, true, mark);
+    }
 }
 
 template <typename R>
@@ -434,19 +503,11 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     ensure_norms<R>(s, n_iter);
     ck(cudaEventRecord(s->ev0, s->stream), "event");
     int64_t launches = 0;
-    for (int it = 0; it < n_iter; ++it) {
-        if (s->sc.order == 2) {
-            Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, states<R>(s)[s->cur], w, s->stream);
-            ++launches;
-        }
-        for (int k = 0; k < s->sc.rk_level; ++k) launches += one_stage<R>(s, k, it, true);
-    }
+    iterations<R>(s, n_iter, [&](int) { ++launches; });
     ck(cudaEventRecord(s->ev1, s->stream), "event");
     ck(cudaGetLastError(), "kernel launch");
-    std::vector<unsigned long long> li((size_t)n_iter * s->nv);
-    std::vector<double> l2((size_t)n_iter * s->nv);
-    ck(cudaMemcpyAsync(li.data(), w.linf, li.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->stream),
-       "norm copy");
+    std::vector<double> li((size_t)n_iter * s->nv), l2((size_t)n_iter * s->nv);
+    ck(cudaMemcpyAsync(li.data(), w.linf, li.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
     ck(cudaMemcpyAsync(l2.data(), w.l2, l2.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
     check_err(s, w.err);
     float ms = 0.0f;
@@ -454,13 +515,39 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     s->last_ms = ms;
     s->last_launches = launches;
     s->iter += n_iter;
-    if (res_linf)
-        for (size_t i = 0; i < li.size(); ++i) {
-            double d;
-            std::memcpy(&d, &li[i], sizeof d);
-            res_linf[i] = d;
-        }
+    if (res_linf) std::memcpy(res_linf, li.data(), li.size() * sizeof(double));
     if (res_l2) std::memcpy(res_l2, l2.data(), l2.size() * sizeof(double));
+}
+
+template <typename R>
+void run_profile(psst_solver *s, int n_iter, double *ms, int64_t *cnt) {
+    DevWork<R> &w = work<R>(s);
+    ensure_norms<R>(s, n_iter);
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    auto mark = [&](int k) {
+        cudaEvent_t e;
+        ck(cudaEventCreate(&e), "event");
+        ck(cudaEventRecord(e, s->stream), "event");
+        ev.push_back(e);
+        kind.push_back(k);
+    };
+    mark(-1);
+    iterations<R>(s, n_iter, mark);
+    ck(cudaGetLastError(), "kernel launch");
+    check_err(s, w.err);
+    for (int k = 0; k < PSST_KERNEL_KINDS; ++k) {
+        ms[k] = 0.0;
+        cnt[k] = 0;
+    }
+    for (size_t i = 1; i < ev.size(); ++i) {
+        float t = 0.0f;
+        ck(cudaEventElapsedTime(&t, ev[i - 1], ev[i]), "event time");
+        ms[kind[i]] += t;
+        cnt[kind[i]] += 1;
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+    s->iter += n_iter;
 }
 
 template <typename R>
@@ -468,17 +555,19 @@ void set_state(psst_solver *s, const double *prim) {
     const int dim = s->dim;
     const int64_t nv = s->nvol_ref;
     const int32_t nall = s->L.nall;
-    std::vector<R> hp(nall), hT(nall), hu((size_t)dim * nall);
+    std::vector<CellRec<R>> h(nall);
     for (int32_t d = 0; d < nall; ++d) {
         const int64_t v = s->L.vol_of_dev[d];
-        hp[d] = (R)prim[v];
-        hT[d] = (R)prim[nv + v];
-        for (int k = 0; k < dim; ++k) hu[(size_t)k * nall + d] = (R)prim[(2 + k) * nv + v];
+        CellRec<R> r;
+        std::memset(&r, 0, sizeof r);
+        r.v[RP] = (R)prim[v];
+        r.v[RT] = (R)prim[nv + v];
+        for (int k = 0; k < dim; ++k) r.v[RU + k] = (R)prim[(2 + k) * nv + v];
+        h[d] = r;
     }
     DevState<R> &st = states<R>(s)[s->cur];
-    ck(cudaMemcpyAsync(st.p, hp.data(), nall * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
-    ck(cudaMemcpyAsync(st.T, hT.data(), nall * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
-    ck(cudaMemcpyAsync(st.u, hu.data(), hu.size() * sizeof(R), cudaMemcpyHostToDevice, s->stream), "state upload");
+    ck(cudaMemcpyAsync(st.rec, h.data(), (size_t)nall * sizeof(CellRec<R>), cudaMemcpyHostToDevice, s->stream),
+       "state upload");
     Ops<R>::prologue(dim, s->g, st, work<R>(s), s->gas, s->stream);
     ck(cudaGetLastError(), "prologue");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
@@ -489,11 +578,10 @@ void get_state(psst_solver *s, double *prim, double *wout) {
     const int dim = s->dim;
     const int64_t nv = s->nvol_ref;
     const int32_t nall = s->L.nall, nint = s->L.nint;
-    std::vector<R> hp(nall), hT(nall), hu((size_t)dim * nall);
+    std::vector<CellRec<R>> h(nall);
     const DevState<R> &st = states<R>(s)[s->cur];
-    ck(cudaMemcpyAsync(hp.data(), st.p, nall * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
-    ck(cudaMemcpyAsync(hT.data(), st.T, nall * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
-    ck(cudaMemcpyAsync(hu.data(), st.u, hu.size() * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "state copy");
+    ck(cudaMemcpyAsync(h.data(), st.rec, (size_t)nall * sizeof(CellRec<R>), cudaMemcpyDeviceToHost, s->stream),
+       "state copy");
     std::vector<double> hw;
     if (wout) {
         hw.resize((size_t)s->nv * nint);
@@ -505,9 +593,9 @@ void get_state(psst_solver *s, double *prim, double *wout) {
         std::fill(prim, prim + (size_t)(2 + dim) * nv, 0.0);
         for (int32_t d = 0; d < nall; ++d) {
             const int64_t v = s->L.vol_of_dev[d];
-            prim[v] = (double)hp[d];
-            prim[nv + v] = (double)hT[d];
-            for (int k = 0; k < dim; ++k) prim[(2 + k) * nv + v] = (double)hu[(size_t)k * nall + d];
+            prim[v] = (double)h[d].v[RP];
+            prim[nv + v] = (double)h[d].v[RT];
+            for (int k = 0; k < dim; ++k) prim[(2 + k) * nv + v] = (double)h[d].v[RU + k];
         }
     }
     if (wout) {
@@ -519,57 +607,80 @@ void get_state(psst_solver *s, double *prim, double *wout) {
     }
 }
 
+template <typename R, int DIM>
+void grad_array(psst_solver *s, const std::string &nm, double *out) {
+    constexpr int NVAR = DIM + 2;
+    const int32_t nint = s->L.nint;
+    std::vector<GradRec<R, DIM>> h(nint);
+    ck(cudaMemcpyAsync(h.data(), work<R>(s).grec, (size_t)nint * sizeof(GradRec<R, DIM>), cudaMemcpyDeviceToHost,
+                       s->stream),
+       "array copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    for (int32_t d = 0; d < nint; ++d) {
+        const int64_t v = s->L.vol_of_dev[d];
+        if (nm == "limiter") {
+            for (int i = 0; i < NVAR; ++i) out[v * NVAR + i] = (double)h[d].lim[i];
+        } else if (nm == "grad_u") {
+            for (int j = 0; j < DIM * DIM; ++j) out[v * DIM * DIM + j] = (double)h[d].g[j];
+        } else {
+            const int var = nm == "grad_p" ? DIM : DIM + 1;
+            for (int k = 0; k < DIM; ++k) out[v * DIM + k] = (double)h[d].g[var * DIM + k];
+        }
+    }
+}
+
 template <typename R>
 void get_array(psst_solver *s, const std::string &nm, double *out, int64_t count) {
     const int dim = s->dim, nvv = s->nv;
     const int64_t nv = s->nvol_ref;
     const int32_t nint = s->L.nint;
     DevWork<R> &w = work<R>(s);
-    auto fetch = [&](const void *src, size_t n, size_t elem) {
-        std::vector<char> h(n * elem);
-        ck(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, s->stream), "array copy");
-        ck(cudaStreamSynchronize(s->stream), "stream sync");
-        return h;
-    };
     auto need = [&](int64_t n) {
         if (n != count) raise(PSST_ERR_ARG, nm + ": expected " + std::to_string(n) + " elements");
         std::fill(out, out + n, 0.0);
     };
     if (nm == "dt") {
         need(nv);
-        auto h = fetch(w.dt, nint, sizeof(double));
-        const double *p = (const double *)h.data();
-        for (int32_t d = 0; d < nint; ++d) out[s->L.vol_of_dev[d]] = p[d];
+        std::vector<double> h(nint);
+        ck(cudaMemcpyAsync(h.data(), w.dt, (size_t)nint * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "copy");
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+        for (int32_t d = 0; d < nint; ++d) out[s->L.vol_of_dev[d]] = h[d];
         return;
     }
-    if (nm == "residual" || nm == "limiter") {
+    if (nm == "residual") {
         need((int64_t)nvv * nv);
-        auto h = fetch(nm == "residual" ? (const void *)w.res : (const void *)w.lim, (size_t)nvv * nint, sizeof(R));
-        const R *p = (const R *)h.data();
+        std::vector<R> h((size_t)nvv * nint);
+        ck(cudaMemcpyAsync(h.data(), w.res, h.size() * sizeof(R), cudaMemcpyDeviceToHost, s->stream), "copy");
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
         for (int32_t d = 0; d < nint; ++d)
-            for (int q = 0; q < nvv; ++q) out[s->L.vol_of_dev[d] * nvv + q] = (double)p[(size_t)q * nint + d];
+            for (int q = 0; q < nvv; ++q) out[s->L.vol_of_dev[d] * nvv + q] = (double)h[(size_t)q * nint + d];
         return;
     }
-    int var = -1, width = dim;
-    if (nm == "grad_u") {
-        var = 0;
-        width = dim * dim;
-    } else if (nm == "grad_p") {
-        var = dim;
-    } else if (nm == "grad_T") {
-        var = dim + 1;
-    }
-    if (var < 0) raise(PSST_ERR_ARG, "unknown solver array " + nm);
-    need((int64_t)width * nv);
-    auto h = fetch(w.grad, (size_t)nvv * dim * nint, sizeof(R));
-    const R *p = (const R *)h.data();
-    for (int32_t d = 0; d < nint; ++d) {
-        const int64_t v = s->L.vol_of_dev[d];
-        for (int j = 0; j < width; ++j) {
-            const int i = var + j / dim, k = j % dim;
-            out[v * width + j] = (double)p[((size_t)i * dim + k) * nint + d];
-        }
-    }
+    int64_t width;
+    if (nm == "limiter")
+        width = nvv;
+    else if (nm == "grad_u")
+        width = (int64_t)dim * dim;
+    else if (nm == "grad_p" || nm == "grad_T")
+        width = dim;
+    else
+        raise(PSST_ERR_ARG, "unknown solver array " + nm);
+    need(width * nv);
+    if (dim == 2)
+        grad_array<R, 2>(s, nm, out);
+    else
+        grad_array<R, 3>(s, nm, out);
+}
+
+template <typename R>
+void stage_api(psst_solver *s, int k, double *res_linf) {
+    ensure_norms<R>(s, 1);
+    one_stage<R>(s, k, 0, false, [](int) {});
+    std::vector<double> li(s->nv);
+    ck(cudaMemcpyAsync(li.data(), work<R>(s).linf, li.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+       "norm copy");
+    check_err(s, work<R>(s).err);
+    if (res_linf) std::memcpy(res_linf, li.data(), li.size() * sizeof(double));
 }
 
 }  // namespace
@@ -639,11 +750,6 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.nall = L.nall;
     g.nface = L.nface;
     g.nfi = L.nfi;
-    g.c0 = s->upload(L.c0);
-    g.c1 = s->upload(L.c1);
-    g.S = s->upload(L.S);
-    g.n = s->upload(L.n);
-    g.xf = s->upload(L.xf);
     g.beta = s->upload(L.beta);
     g.V = s->upload(L.V);
     g.xc = s->upload(L.xc);
@@ -653,6 +759,7 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.lsq_r = s->upload(L.lsq_r);
     g.vk_eps2 = s->upload(L.vk_eps2);
     g.rank = s->upload(L.rank);
+    g.gptr = s->upload(L.gptr);
     g.g_nb = s->upload(L.g_nb);
     g.g_face = s->upload(L.g_face);
     g.g_zone = s->upload(L.g_zone);
@@ -665,9 +772,9 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.lvl_ptr = s->upload(L.lvl_ptr);
     g.nlevels = L.nlevels;
     if (sc->precision == 32)
-        alloc_state<float>(s.get());
+        alloc_state<float>(s.get(), *G);
     else
-        alloc_state<double>(s.get());
+        alloc_state<double>(s.get(), *G);
     ck(cudaDeviceSynchronize(), "setup");
     *out = s.release();
     PSST_API_END
@@ -711,33 +818,20 @@ extern "C" psst_status psst_convective_calculate(psst_solver *s) {
     if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     if (s->sc.precision == 32) {
-        Ops<float>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, s->s32[s->cur], s->w32, s->gas, s->stream);
+        Ops<float>::face(s->dim, s->sc.flux, s->rec, s->sc.limiter, 0, s->g, s->s32[s->cur], s->w32, s->gas,
+                         s->stream);
         Ops<float>::residual(s->dim, s->g, s->w32, s->stream);
+        ck(cudaGetLastError(), "convective");
         check_err(s, s->w32.err);
     } else {
-        Ops<double>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, s->s64[s->cur], s->w64, s->gas,
-                               s->stream);
+        Ops<double>::face(s->dim, s->sc.flux, s->rec, s->sc.limiter, 0, s->g, s->s64[s->cur], s->w64, s->gas,
+                          s->stream);
         Ops<double>::residual(s->dim, s->g, s->w64, s->stream);
+        ck(cudaGetLastError(), "convective");
         check_err(s, s->w64.err);
     }
-    ck(cudaGetLastError(), "convective");
     PSST_API_END
 }
-
-namespace {
-template <typename R>
-void stage_api(psst_solver *s, int k, double *res_linf) {
-    ensure_norms<R>(s, 1);
-    one_stage<R>(s, k, 0, false);
-    std::vector<unsigned long long> li(s->nv);
-    ck(cudaMemcpyAsync(li.data(), work<R>(s).linf, li.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                       s->stream),
-       "norm copy");
-    check_err(s, work<R>(s).err);
-    if (res_linf)
-        for (int i = 0; i < s->nv; ++i) std::memcpy(&res_linf[i], &li[i], sizeof(double));
-}
-}  // namespace
 
 extern "C" psst_status psst_stage_update(psst_solver *s, int k, double *res_linf) {
     PSST_API_BEGIN
@@ -782,58 +876,6 @@ extern "C" psst_status psst_solver_last_stats(const psst_solver *s, int64_t *lau
     if (device_ms) *device_ms = s->last_ms;
     PSST_API_END
 }
-
-namespace {
-template <typename R>
-void run_profile(psst_solver *s, int n_iter, double *ms, int64_t *cnt) {
-    DevWork<R> &w = work<R>(s);
-    ensure_norms<R>(s, n_iter);
-    std::vector<cudaEvent_t> ev;
-    std::vector<int> kind;
-    auto mark = [&](int k) {
-        cudaEvent_t e;
-        ck(cudaEventCreate(&e), "event");
-        ck(cudaEventRecord(e, s->stream), "event");
-        ev.push_back(e);
-        kind.push_back(k);
-    };
-    DevState<R> *st = states<R>(s);
-    mark(-1);
-    for (int it = 0; it < n_iter; ++it) {
-        if (s->sc.order == 2) {
-            Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, st[s->cur], w, s->stream);
-            mark(0);
-        }
-        for (int k = 0; k < s->sc.rk_level; ++k) {
-            const DevState<R> &cur = st[s->cur], &nxt = st[s->cur ^ 1];
-            Ops<R>::face_flux(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->g, cur, w, s->gas, s->stream);
-            mark(1);
-            Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, true, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
-                                s->sc.rk[k], k == 0, it, s->stream);
-            mark(2);
-            Ops<R>::ghost_update(s->dim, s->g, cur, nxt, s->gas, s->stream);
-            mark(3);
-            Ops<R>::l2_finish(s->dim, w, s->seq ? 1 : s->nblk, s->L.nint, it, s->stream);
-            mark(4);
-            s->cur ^= 1;
-        }
-    }
-    ck(cudaGetLastError(), "kernel launch");
-    check_err(s, w.err);
-    for (int k = 0; k < PSST_KERNEL_KINDS; ++k) {
-        ms[k] = 0.0;
-        cnt[k] = 0;
-    }
-    for (size_t i = 1; i < ev.size(); ++i) {
-        float t = 0.0f;
-        ck(cudaEventElapsedTime(&t, ev[i - 1], ev[i]), "event time");
-        ms[kind[i]] += t;
-        cnt[kind[i]] += 1;
-    }
-    for (auto e : ev) cudaEventDestroy(e);
-    s->iter += n_iter;
-}
-}  // namespace
 
 extern "C" psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind) {
     PSST_API_BEGIN

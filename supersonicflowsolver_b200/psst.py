@@ -188,7 +188,7 @@ class Solver:
         check(_lib.load().psst_solver_get_array(self._h, name.encode(), _ptr(out), out.size))
         return out
 
-    KERNEL_KINDS = ("gradient", "face_flux", "cell_update", "ghost_update", "norm_finish")
+    KERNEL_KINDS = ("gradient", "face", "cell", "ghost_update", "norm_finish")
 
     def profile(self, n_iter):
         """n iterations with a CUDA event pair around every launch; returns
