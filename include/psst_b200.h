@@ -227,6 +227,49 @@ psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, doub
 #define PSST_KERNEL_KINDS 5
 psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind);
 
+/* ------------------------------------------------------------------------ */
+/* Residual without any allocation                                           */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory -- code running under an application or framework that owns every
+ * device allocation (a pool or arena it hands out), or a solver embedded in a
+ * host that forbids growing the device footprint after start-up -- and so
+ * cannot create a solver object, since psst_solver_create allocates.
+ *
+ * Computes the first-order convective residual (the result of
+ * psst_convective_calculate for order 1: HLL/HLLC/AUSM fluxes of unreconstructed
+ * cell states, ghost physical flux on boundary faces, per-cell sums in the
+ * order of each cell's CSR) from caller-owned DEVICE arrays into a
+ * caller-owned device array. It calls no cudaMalloc/cudaFree and no allocating
+ * library routine: the per-face flux buffer it needs is a fixed array compiled
+ * into the library, sized for PSST_STATIC_MAX_FACES faces (5.24 MB, held on
+ * every GPU that loads the library until the process exits). Larger meshes are
+ * rejected with PSST_ERR_ARG.
+ *
+ *  volumes: interior cells are [0, nint), ghost cells [nint, nall);
+ *  face_c0/face_c1 [nface]: neighbour volumes (a face with a ghost side is a
+ *    boundary face); face_S [nface]; face_n [dim][nface] unit normals pointing
+ *    from neighbour 1 into neighbour 0;
+ *  csr_ptr [nint+1], csr_ent: per interior cell, (face << 1 | side) entries in
+ *    the order the residual is summed (the reference's face-loop order);
+ *  prim [(3+dim)][nall]: p, T, rho, u0, u1, (u2);
+ *  residual [(dim+2)][nint] (output): rho*u.., rho, rho*E components.
+ *
+ * The first call on a device looks up the device address of the fixed buffer
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. Every call shares the buffer and it keeps the
+ * last call's contents; calls that overlap on the GPU (on different streams or
+ * threads) race on it. The call synchronises `stream` (a cudaStream_t, NULL =
+ * legacy default stream) to report a failed wave-speed ordering as
+ * PSST_ERR_FLUX, like psst_convective_calculate. */
+#define PSST_STATIC_MAX_FACES 131072
+psst_status psst_convective_residual_static(int32_t dim, int32_t flux, int32_t nint, int32_t nall, int32_t nface,
+                                            const int32_t *face_c0, const int32_t *face_c1, const double *face_S,
+                                            const double *face_n, const int32_t *csr_ptr, const int32_t *csr_ent,
+                                            const double *prim, double rm, double cp, double cv, double gamma,
+                                            double *residual, void *stream);
+
 /* Reference counter psstGridFV::iter_ after the calls so far. */
 int64_t psst_solver_iter(const psst_solver *s);
 

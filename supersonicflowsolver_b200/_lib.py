@@ -23,7 +23,7 @@ EXPORTED = [
     "psst_gradient_calculate", "psst_convective_calculate", "psst_stage_update", "psst_explicit_solve",
     "psst_solver_get_array", "psst_solver_set_stream", "psst_solver_last_stats", "psst_solver_profile",
     "psst_solver_iter",
-    "psst_solver_destroy",
+    "psst_solver_destroy", "psst_convective_residual_static",
 ]
 
 
@@ -105,6 +105,7 @@ def load():
         "psst_solver_profile": (I, [P, I, P, P]),
         "psst_solver_iter": (I64, [P]),
         "psst_solver_destroy": (None, [P]),
+        "psst_convective_residual_static": (I, [ctypes.c_int32] * 5 + [P] * 7 + [D] * 4 + [P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
