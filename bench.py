@@ -280,6 +280,7 @@ def run_gpu(args):
     solver.set_stream(stream.cuda_stream)
     solver.set_state(prim)
     nint = grid.ninterior
+    shapes = solver.autotune(2) if not args.no_autotune else solver.launch_shape()
 
     def barrier():
         if ws > 1:
@@ -345,6 +346,7 @@ def run_gpu(args):
                                  "(stage-start values), CFL 0.5, Mach 3, 12 deg ramp",
                        "precision": "FP32 state/flux; FP64 geometry, RK state, residual norms",
                        "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "threads_per_block": shapes,
                        "l2_flush": "not needed: >2.5 GB of mesh + state per step, L2 is 126 MB"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": state_bytes / args.steps,
@@ -382,6 +384,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wedge3d_6M_tets", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -227,6 +227,21 @@ psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, doub
 #define PSST_KERNEL_KINDS 5
 psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind);
 
+/* No counterpart in the reference (its loop is serial). Launch-shape tuner:
+ * times n_iter iterations at 64, 128 and 256 threads per block on the
+ * solver's own mesh and state, keeps the fastest shape for each of the
+ * gradient, face and cell passes, and restores the state and iteration count,
+ * so the next psst_explicit_solve continues from where it was. blocks (may be
+ * NULL) receives the chosen shapes {gradient, face, cell}. The shapes change
+ * no result except the last bits of the RMS column (its block partials follow
+ * the cell-pass shape). Allocates a state-sized snapshot for the call. */
+psst_status psst_solver_autotune(psst_solver *s, int n_iter, int *blocks);
+
+/* Sets (set != NULL; 0 keeps an entry) and/or reads (get != NULL) the launch
+ * shapes {gradient, face, cell}: 64, 128 or 256 threads per block (default
+ * 256). */
+psst_status psst_solver_launch_shape(psst_solver *s, const int *set, int *get);
+
 /* ------------------------------------------------------------------------ */
 /* Residual without any allocation                                           */
 /* ------------------------------------------------------------------------ */

@@ -22,7 +22,7 @@ EXPORTED = [
     "psst_grid_set_boundary", "psst_solver_create", "psst_solver_set_state", "psst_solver_get_state",
     "psst_gradient_calculate", "psst_convective_calculate", "psst_stage_update", "psst_explicit_solve",
     "psst_solver_get_array", "psst_solver_set_stream", "psst_solver_last_stats", "psst_solver_profile",
-    "psst_solver_iter",
+    "psst_solver_autotune", "psst_solver_launch_shape", "psst_solver_iter",
     "psst_solver_destroy", "psst_convective_residual_static",
 ]
 
@@ -103,6 +103,8 @@ def load():
         "psst_solver_set_stream": (I, [P, P]),
         "psst_solver_last_stats": (I, [P, ctypes.POINTER(I64), ctypes.POINTER(D)]),
         "psst_solver_profile": (I, [P, I, P, P]),
+        "psst_solver_autotune": (I, [P, I, P]),
+        "psst_solver_launch_shape": (I, [P, P, P]),
         "psst_solver_iter": (I64, [P]),
         "psst_solver_destroy": (None, [P]),
         "psst_convective_residual_static": (I, [ctypes.c_int32] * 5 + [P] * 7 + [D] * 4 + [P, P]),

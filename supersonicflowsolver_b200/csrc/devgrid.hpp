@@ -74,6 +74,9 @@ struct DevGrid {
     const int32_t *lvl_cells; // [nint] cells grouped by level (sequential LocalAccTime1)
     const int32_t *lvl_ptr;   // [nlevels+1]
     int32_t nlevels;
+    // launch shapes (threads per block: 64, 128 or 256) of the gradient, face
+    // and cell passes; set by the solver, tuned by psst_solver_autotune
+    int32_t blk_grad, blk_face, blk_cell;
 };
 
 template <typename R>

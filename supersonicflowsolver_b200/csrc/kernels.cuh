@@ -398,13 +398,26 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
 #pragma unroll
         for (int k = 0; k < DIM; ++k) gr[i][k] = (R)0;
     const uint64_t perm = g.wperm[c];
+    // min/max of each variable over the face neighbours for limiters 4/5
+    // (order-free), gathered in the same pass as the gradient
+    R mx[NVAR], mn[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) mx[i] = mn[i] = pvar<R, DIM>(own, i);
     if (GRAD == 1) {
         const double V = g.V[c];
+#pragma unroll 4
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
             const FaceRec<R, DIM> fr = ld16(frec + f);
             const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + (side ? fr.c0 : fr.c1)));
+            if (CELLLIM)
+#pragma unroll
+                for (int i = 0; i < NVAR; ++i) {
+                    const R v = pvar<R, DIM>(oth, i);
+                    if (v > mx[i]) mx[i] = v;
+                    if (v < mn[i]) mn[i] = v;
+                }
             const R beta = (R)g.beta[f];
             const R rbeta = (R)1 - beta;
             const R gp = (R)(fr.S / V);
@@ -427,6 +440,13 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
             const FaceRec<R, DIM> fr = ld16(frec + f);
             const int32_t nb = (ent & 1) ? fr.c0 : fr.c1;
             const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + nb));
+            if (CELLLIM)
+#pragma unroll
+                for (int i = 0; i < NVAR; ++i) {
+                    const R v = pvar<R, DIM>(oth, i);
+                    if (v > mx[i]) mx[i] = v;
+                    if (v < mn[i]) mn[i] = v;
+                }
             R diff[2];
             diff[0] = (R)g.xc[nb] - xc0;
             diff[1] = (R)g.xc[(int64_t)g.nall + nb] - xc1;
@@ -454,20 +474,7 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
     }
     if (CELLLIM) {
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
-        R mx[NVAR], mn[NVAR];
-#pragma unroll
-        for (int i = 0; i < NVAR; ++i) mx[i] = mn[i] = pvar<R, DIM>(own, i);
-        for (int32_t q = 0; q < K; ++q) {  // min/max over the face neighbours (order-free)
-            const int32_t ent = g.csr_ent[b + q];
-            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
-            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + ((ent & 1) ? fr.c0 : fr.c1)));
-#pragma unroll
-            for (int i = 0; i < NVAR; ++i) {
-                const R v = pvar<R, DIM>(oth, i);
-                if (v > mx[i]) mx[i] = v;
-                if (v < mn[i]) mn[i] = v;
-            }
-        }
+#pragma unroll 4
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
             const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
@@ -758,15 +765,49 @@ __global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevSta
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
     if (c < g.nint) {
         const FO *fo = reinterpret_cast<const FO *>(wk.fout);
+        const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+        const uint64_t perm = g.wperm[c];
+        // When the cell's own face order is the face-loop order (the usual
+        // case: faces are wired zone by zone in file order, and files list
+        // zones in ascending id), residual and time step share one pass.
+        const bool one_pass = LC != 0 && perm == (0xFEDCBA9876543210ull & ((K >= 16) ? ~0ull : ((1ull << (4 * K)) - 1)));
         R res[NV];
-        gather_residual<R, DIM>(g, fo, c, res);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) res[v] = (R)0;
+        R den = (R)0, nnb = (R)0, s[DIM];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s[k] = (R)0;
+#pragma unroll 4
+        for (int32_t q = 0; q < K; ++q) {
+            const int32_t ent = g.csr_ent[b + q];
+            const FO o = ld16(fo + (ent >> 1));
+            const int side = ent & 1;
+            if (side) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) res[v] += o.v[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) res[v] -= o.v[v];
+            }
+            if (one_pass) {
+                if (LC == 1) {
+                    R nv = (R)0;
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) {
+                        nv += side ? o.v[FO::Q1 + k] : o.v[FO::Q0 + k];
+                        nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];
+                    }
+                    nnb = (nnb + nv) * (R)0.5;
+                    den += (fabs(nnb) + o.v[FO::CN]) * o.v[FO::SA];
+                } else if (LC == 2) {
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
+                }
+            }
+        }
         double dt = dt_uniform;
         if (LC != 0) {
-            const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
-            const uint64_t perm = g.wperm[c];
-            R den = (R)0;
-            if (LC == 1) {
-                R nnb = (R)0;
+            if (LC == 1 && !one_pass) {  // the cell's own face order differs: second pass
                 for (int32_t j = 0; j < K; ++j) {
                     const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
                     const FO o = ld16(fo + (ent >> 1));
@@ -780,16 +821,14 @@ __global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevSta
                     nnb = (nnb + nv) * (R)0.5;
                     den += (fabs(nnb) + o.v[FO::CN]) * o.v[FO::SA];
                 }
-            } else {
-                R s[DIM];
+            } else if (LC == 2) {
+                if (!one_pass)
+                    for (int32_t j = 0; j < K; ++j) {
+                        const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+                        const FO o = ld16(fo + (ent >> 1));
 #pragma unroll
-                for (int k = 0; k < DIM; ++k) s[k] = (R)0;
-                for (int32_t j = 0; j < K; ++j) {
-                    const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
-                    const FO o = ld16(fo + (ent >> 1));
-#pragma unroll
-                    for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
-                }
+                        for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
+                    }
                 const Prim<R, DIM> own = unpack<R, DIM>(ld16(cur.rec + c));
                 const R cc = sqrt((R)gas.gamma * (R)gas.rm * own.T);
 #pragma unroll

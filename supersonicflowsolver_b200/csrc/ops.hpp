@@ -10,6 +10,7 @@
 namespace psst {
 
 constexpr int kBlock = 256;
+constexpr int kMinBlock = 64;  // smallest launch shape the tuner may pick
 inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
 template <typename R>

@@ -32,21 +32,21 @@ void Ops<R>::prologue(int dim, const DevGrid &g, const DevState<R> &st, const De
 template <typename R, int DIM>
 static void gradient_dim(int grad, int celllim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
                          cudaStream_t s) {
-    const int nb = nblocks(g.nint);
+    const int bs = g.blk_grad, nb = nblocks(g.nint, bs);
     if (grad == 1) {
         if (celllim == 4)
-            k_gradient<R, DIM, 1, 4><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 1, 4><<<nb, bs, 0, s>>>(g, st, wk);
         else if (celllim == 5)
-            k_gradient<R, DIM, 1, 5><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 1, 5><<<nb, bs, 0, s>>>(g, st, wk);
         else
-            k_gradient<R, DIM, 1, 0><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 1, 0><<<nb, bs, 0, s>>>(g, st, wk);
     } else if (DIM == 2) {
         if (celllim == 4)
-            k_gradient<R, 2, 2, 4><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, 2, 2, 4><<<nb, bs, 0, s>>>(g, st, wk);
         else if (celllim == 5)
-            k_gradient<R, 2, 2, 5><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, 2, 2, 5><<<nb, bs, 0, s>>>(g, st, wk);
         else
-            k_gradient<R, 2, 2, 0><<<nb, kBlock, 0, s>>>(g, st, wk);
+            k_gradient<R, 2, 2, 0><<<nb, bs, 0, s>>>(g, st, wk);
     }
 }
 
@@ -64,13 +64,13 @@ void Ops<R>::gradient(int dim, int grad, int celllim, const DevGrid &g, const De
 template <typename R, int DIM, int FLUX, int REC, int LIM>
 static void face_l(int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
                    cudaStream_t s) {
-    const int nb = nblocks(g.nface);
+    const int bs = g.blk_face, nb = nblocks(g.nface, bs);
     if (lc == 1)
-        k_face<R, DIM, FLUX, REC, LIM, 1><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+        k_face<R, DIM, FLUX, REC, LIM, 1><<<nb, bs, 0, s>>>(g, st, wk, gas);
     else if (lc == 2)
-        k_face<R, DIM, FLUX, REC, LIM, 2><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+        k_face<R, DIM, FLUX, REC, LIM, 2><<<nb, bs, 0, s>>>(g, st, wk, gas);
     else
-        k_face<R, DIM, FLUX, REC, LIM, 0><<<nb, kBlock, 0, s>>>(g, st, wk, gas);
+        k_face<R, DIM, FLUX, REC, LIM, 0><<<nb, bs, 0, s>>>(g, st, wk, gas);
 }
 
 template <typename R, int DIM, int FLUX>
@@ -113,13 +113,13 @@ void Ops<R>::face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g,
 template <typename R, int DIM>
 static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const DevWork<R> &wk,
                    const Gas &gas, double cfl, double dtu, double alpha, int first, int it, cudaStream_t s) {
-    const int nb = nblocks(g.nint);
+    const int bs = g.blk_cell, nb = nblocks(g.nint, bs);
     if (lc == 1)
-        k_cell<R, DIM, 1><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 1><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
     else if (lc == 2)
-        k_cell<R, DIM, 2><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 2><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
     else
-        k_cell<R, DIM, 0><<<nb, kBlock, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 0><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
 }
 
 template <typename R>

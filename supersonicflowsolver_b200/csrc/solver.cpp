@@ -411,7 +411,8 @@ void alloc_state(psst_solver *s, const psst_grid &G) {
     w.fout = s->dalloc_bytes(Ops<R>::face_out_bytes(dim) * std::max(nface, 1));
     w.res = s->dalloc<R>((size_t)nv * nint);
     w.dt = s->dalloc<double>(nint);
-    w.l2part = s->dalloc<double>((size_t)2 * nv * std::max(s->nblk, 1));
+    // sized for the smallest cell-pass block (64 threads): one partial per block
+    w.l2part = s->dalloc<double>((size_t)2 * nv * std::max(nblocks(nint, kMinBlock), 1));
     w.ticket = s->dalloc<unsigned int>(1);
     w.err = s->dalloc<int32_t>(4);
     ck(cudaMemset(w.grec, 0, gbytes * std::max(nint, 1)), "memset");
@@ -548,6 +549,69 @@ void run_profile(psst_solver *s, int n_iter, double *ms, int64_t *cnt) {
     }
     for (auto e : ev) cudaEventDestroy(e);
     s->iter += n_iter;
+}
+
+// Launch-shape tuner: runs n_iter iterations per candidate block size on the
+// solver's own mesh and state, times each pass with events, keeps the fastest
+// shape per pass, and puts the state back (device-to-device snapshot of the
+// primitive records and the conservative state; everything else a stage reads
+// is recomputed from those), so the solution and the iteration count are
+// unchanged. Results do not depend on the shapes except for the rounding of
+// the RMS column, whose block partials follow the cell-pass shape.
+template <typename R>
+void autotune(psst_solver *s, int n_iter, int *blocks) {
+    DevState<R> *st = states<R>(s);
+    DevWork<R> &w = work<R>(s);
+    const size_t rb = (size_t)std::max(s->L.nall, 1) * sizeof(CellRec<R>);
+    const size_t wb = (size_t)s->nv * std::max(s->L.nint, 1) * sizeof(double);
+    void *snap = nullptr;
+    ck(cudaMalloc(&snap, rb + wb), "cudaMalloc");
+    const int cur0 = s->cur;
+    const int64_t iter0 = s->iter;
+    auto copy = [&](bool save) {
+        void *r = st[cur0].rec, *ww = w.w, *sr = snap, *sw = (char *)snap + rb;
+        ck(cudaMemcpyAsync(save ? sr : r, save ? r : sr, rb, cudaMemcpyDeviceToDevice, s->stream), "snapshot");
+        ck(cudaMemcpyAsync(save ? sw : ww, save ? ww : sw, wb, cudaMemcpyDeviceToDevice, s->stream), "snapshot");
+    };
+    const int cand[3] = {64, 128, 256};
+    const int kinds[3] = {K_GRADIENT, K_FACE, K_CELL};
+    double best[3] = {1e300, 1e300, 1e300};
+    int pick[3] = {s->g.blk_grad, s->g.blk_face, s->g.blk_cell};
+    try {
+        copy(true);
+        for (int b : cand) {
+            s->g.blk_grad = s->g.blk_face = s->g.blk_cell = b;
+            double ms[PSST_KERNEL_KINDS];
+            int64_t cnt[PSST_KERNEL_KINDS];
+            run_profile<R>(s, 1, ms, cnt);  // warm-up at this shape
+            copy(false);
+            s->cur = cur0;
+            run_profile<R>(s, n_iter, ms, cnt);
+            copy(false);
+            s->cur = cur0;
+            for (int i = 0; i < 3; ++i)
+                if (cnt[kinds[i]] > 0 && ms[kinds[i]] / cnt[kinds[i]] < best[i]) {
+                    best[i] = ms[kinds[i]] / cnt[kinds[i]];
+                    pick[i] = b;
+                }
+        }
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+    } catch (...) {
+        cudaMemcpyAsync(st[cur0].rec, snap, rb, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(w.w, (char *)snap + rb, wb, cudaMemcpyDeviceToDevice, s->stream);
+        cudaStreamSynchronize(s->stream);
+        cudaFree(snap);
+        s->cur = cur0;
+        s->iter = iter0;
+        throw;
+    }
+    cudaFree(snap);
+    s->iter = iter0;
+    s->g.blk_grad = pick[0];
+    s->g.blk_face = pick[1];
+    s->g.blk_cell = pick[2];
+    if (blocks)
+        for (int i = 0; i < 3; ++i) blocks[i] = pick[i];
 }
 
 template <typename R>
@@ -771,6 +835,7 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.lvl_cells = s->upload(L.lvl_cells);
     g.lvl_ptr = s->upload(L.lvl_ptr);
     g.nlevels = L.nlevels;
+    g.blk_grad = g.blk_face = g.blk_cell = kBlock;
     if (sc->precision == 32)
         alloc_state<float>(s.get(), *G);
     else
@@ -884,6 +949,35 @@ extern "C" psst_status psst_solver_profile(psst_solver *s, int n_iter, double *m
     if (n_iter <= 0) raise(PSST_ERR_ARG, "n_iter must be positive");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     DISPATCH(s, run_profile)(s, n_iter, ms_per_kind, launches_per_kind);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_autotune(psst_solver *s, int n_iter, int *blocks) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    if (n_iter <= 0) raise(PSST_ERR_ARG, "n_iter must be positive");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, autotune)(s, n_iter, blocks);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_launch_shape(psst_solver *s, const int *set, int *get) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (set) {
+        for (int i = 0; i < 3; ++i)
+            if (set[i] != 0 && set[i] != 64 && set[i] != 128 && set[i] != 256)
+                raise(PSST_ERR_ARG, "launch shape must be 0 (keep), 64, 128 or 256 threads per block");
+        if (set[0]) s->g.blk_grad = set[0];
+        if (set[1]) s->g.blk_face = set[1];
+        if (set[2]) s->g.blk_cell = set[2];
+    }
+    if (get) {
+        get[0] = s->g.blk_grad;
+        get[1] = s->g.blk_face;
+        get[2] = s->g.blk_cell;
+    }
     PSST_API_END
 }
 

@@ -198,6 +198,21 @@ class Solver:
         check(_lib.load().psst_solver_profile(self._h, int(n_iter), _ptr(ms), _ptr(cnt)))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_KINDS)}
 
+    def autotune(self, n_iter=3):
+        """Times n_iter iterations at each launch shape (64/128/256 threads per
+        block), keeps the fastest per pass and restores the state; returns
+        {"gradient": b, "face": b, "cell": b}."""
+        out = np.zeros(3, dtype=np.int32)
+        check(_lib.load().psst_solver_autotune(self._h, int(n_iter), _ptr(out)))
+        return dict(zip(("gradient", "face", "cell"), (int(x) for x in out)))
+
+    def launch_shape(self, gradient=0, face=0, cell=0):
+        """Sets the launch shapes (0 keeps one) and returns the current ones."""
+        st = np.array([gradient, face, cell], dtype=np.int32)
+        out = np.zeros(3, dtype=np.int32)
+        check(_lib.load().psst_solver_launch_shape(self._h, _ptr(st), _ptr(out)))
+        return dict(zip(("gradient", "face", "cell"), (int(x) for x in out)))
+
     def set_stream(self, stream_ptr):
         check(_lib.load().psst_solver_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 

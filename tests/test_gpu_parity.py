@@ -163,6 +163,40 @@ def test_stage_api_equals_fused_iteration(tmp_path, lc, mesh):
     assert np.all(np.isfinite(res0))
 
 
+@pytest.mark.parametrize("mesh,limiter", [("q", 3), ("t", 5)], ids=["2d_vanleer", "3d_venkat"])
+def test_launch_shapes_and_autotune_keep_results(tmp_path, mesh, limiter):
+    """Every launch shape gives the oracle's state and L-inf column bit for bit
+    (the RMS column to rounding), and the tuner leaves state and iteration
+    count where they were."""
+    m = MESH[mesh]()
+    path, d, name = make_case(tmp_path, m, max_iter=6, flux=3, order=2, limiter=limiter, lc=1,
+                              mach=3.0 if m.dim == 3 else 2.5)
+    o = Oracle(path, d, name, lc1_jacobi=1)
+    olinf, ol2 = o.run(3)
+    for shape in (64, 128, 256):
+        g, s = gpu_solver(path, d, name, lc1_mode=1)
+        assert s.launch_shape(shape, shape, shape) == {"gradient": shape, "face": shape, "cell": shape}
+        linf, l2 = s.explicit_solve(3)
+        assert np.array_equal(linf, olinf)
+        np.testing.assert_allclose(l2, ol2, rtol=1e-12, atol=0)
+        assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim))
+    g, s = gpu_solver(path, d, name, lc1_mode=1)
+    s.explicit_solve(1)
+    before = s.get_state(with_w=True)
+    it = s.iter
+    pick = s.autotune(2)
+    assert set(pick.values()) <= {64, 128, 256}
+    assert s.launch_shape() == pick
+    assert s.iter == it
+    after = s.get_state(with_w=True)
+    for a, b in zip(before, after):
+        assert np.array_equal(a, b)
+    s.explicit_solve(2)
+    assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim))
+    with pytest.raises(PsstError):
+        s.launch_shape(96, 0, 0)
+
+
 def test_deterministic(tmp_path):
     m = MESH["t"]()
     path, d, name = make_case(tmp_path, m, max_iter=5, flux=3, order=2, limiter=5, lc=1, mach=3.0)
