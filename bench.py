@@ -153,14 +153,14 @@ def traffic_model(grid, nnz, kind):
 
 
 def read_traffic(kernel, workload):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/<kernel>_<workload>.txt, line 'dram_bytes_per_launch_full_size: N')."""
-    path = os.path.join(ROOT, "profiles", "%s_%s.txt" % (kernel, workload))
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("dram_bytes_per_launch_full_size:"):
-            return float(line.split(":")[1])
+    """DRAM bytes (read + write) per launch of k_<kernel> on `workload` from the
+    committed ncu summaries: a line 'dram_bytes_per_launch[<workload>]: N' in
+    profiles/k_<kernel>_*.txt."""
+    tag = "dram_bytes_per_launch[%s]:" % workload
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "k_%s_*.txt" % kernel))):
+        for line in open(path):
+            if line.startswith(tag):
+                return float(line.split(":")[1].split()[0])
     return None
 
 

@@ -115,6 +115,27 @@ psst_status psst_grid_get_array(const psst_grid *g, const char *name, void *out,
 
 void psst_grid_free(psst_grid *g);
 
+/* No counterpart in the reference (it solves one case per process). Merges n
+ * case grids, each already set up by psst_case_read, into one grid that is
+ * their disjoint union, so that one solver advances all of them with every
+ * launch. Volumes, faces and zones follow case after case, each case in its
+ * own reference order; zone id z of case i becomes i*1000000 + z and its name
+ * gets "#i". Each case keeps its own geometry, boundary values and initial
+ * state (returned in the merged prim layout by psst_case_read's holder), so
+ * it evolves as it would alone. The inputs stay owned by the caller. Merged
+ * grids need Green-Gauss gradients (the reference's least-squares table is
+ * indexed across zones) and, for LocalAccTime1, lc1_mode JACOBI. */
+psst_status psst_grid_merge(const psst_grid *const *grids, int32_t n, psst_grid **out);
+
+/* Number of cases of a grid (1 unless merged) and, if case_vol_ptr is not
+ * NULL, the ncase+1 volume offsets of the cases. */
+psst_status psst_grid_case_count(const psst_grid *g, int32_t *ncase, int64_t *case_vol_ptr);
+
+/* Initial state of a merged grid in the prim layout of psst_solver_set_state
+ * (the cases' psst_case_read states, concatenated per variable); count =
+ * (2+dim)*nvol. */
+psst_status psst_grid_initial_state(const psst_grid *g, double *prim, int64_t count);
+
 /* ------------------------------------------------------------------------ */
 /* Case setup                                                                */
 /* ------------------------------------------------------------------------ */
@@ -286,6 +307,23 @@ psst_status psst_convective_residual_static(int32_t dim, int32_t flux, int32_t n
                                             double *residual, void *stream);
 
 /* Reference counter psstGridFV::iter_ after the calls so far. */
+/* No counterpart in the reference. With on != 0, each psst_explicit_solve
+ * call is captured once as a CUDA graph (per iteration count and state-buffer
+ * parity) and replayed afterwards: one launch per call instead of one per
+ * kernel, for meshes small enough that launch latency dominates. Changing the
+ * launch shapes drops the captured graphs. */
+psst_status psst_solver_use_graphs(psst_solver *s, int on);
+
+/* Merged grids only. Sets the run flag of every case (active[ncase], non-zero =
+ * run): kernels skip the cells and faces of stopped cases, which keep their
+ * state, and their residual columns read 0. */
+psst_status psst_solver_set_active(psst_solver *s, const int32_t *active);
+
+/* Merged grids only. Per-case residual columns of the last psst_explicit_solve
+ * call: out[n_iter][ncase][dim+2], each the max over RK stages and the case's
+ * cells of |res| (the reference's column, per case). n_iter <= that call's. */
+psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, double *out);
+
 int64_t psst_solver_iter(const psst_solver *s);
 
 void psst_solver_destroy(psst_solver *s);

@@ -24,6 +24,8 @@ EXPORTED = [
     "psst_solver_get_array", "psst_solver_set_stream", "psst_solver_last_stats", "psst_solver_profile",
     "psst_solver_autotune", "psst_solver_launch_shape", "psst_solver_iter",
     "psst_solver_destroy", "psst_convective_residual_static",
+    "psst_grid_merge", "psst_grid_case_count", "psst_grid_initial_state",
+    "psst_solver_use_graphs", "psst_solver_set_active", "psst_solver_case_residuals",
 ]
 
 
@@ -108,6 +110,12 @@ def load():
         "psst_solver_iter": (I64, [P]),
         "psst_solver_destroy": (None, [P]),
         "psst_convective_residual_static": (I, [ctypes.c_int32] * 5 + [P] * 7 + [D] * 4 + [P, P]),
+        "psst_grid_merge": (I, [P, ctypes.c_int32, ctypes.POINTER(P)]),
+        "psst_grid_case_count": (I, [P, P, P]),
+        "psst_grid_initial_state": (I, [P, P, I64]),
+        "psst_solver_use_graphs": (I, [P, I]),
+        "psst_solver_set_active": (I, [P, P]),
+        "psst_solver_case_residuals": (I, [P, I, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

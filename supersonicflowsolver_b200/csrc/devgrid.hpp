@@ -60,6 +60,7 @@ struct DevGrid {
     const double *xc;         // [dim][nall] centroid (ghost: its face centre); least squares only
     const int32_t *csr_ptr;   // [nint+1]
     const int32_t *csr_ent;   // face << 1 | side, sorted by the reference's face-loop order
+    const int32_t *csr_nb;    // the cell across each csr_ent face (saves a dependent load)
     const uint64_t *wperm;    // [nint] 4-bit slots: k-th face of the cell's own face order
     const double *lsq_r;      // [3][nint] 2D least-squares coefficients (reference table)
     const double *vk_eps2;    // [nint] Venkatakrishnan epsilon^2 = (K h)^3, h = V^(1/dim)
@@ -77,6 +78,11 @@ struct DevGrid {
     // launch shapes (threads per block: 64, 128 or 256) of the gradient, face
     // and cell passes; set by the solver, tuned by psst_solver_autotune
     int32_t blk_grad, blk_face, blk_cell;
+    // merged grids only (null otherwise): case of every cell (ghosts included)
+    // and the per-case run flag; cells of a stopped case keep their state
+    int32_t ncase;
+    const int32_t *cell_case;    // [nall]
+    const int32_t *case_active;  // [ncase]
 };
 
 template <typename R>
@@ -96,6 +102,8 @@ struct DevWork {
     double *l2part;      // [nblocks][2][dim+2] per-block sum of res^2 and max |res|
     unsigned int *ticket;  // [1] blocks finished in the current launch
     int32_t *err;        // [4] error word, face id, cell id, code
+    unsigned long long *case_linf;  // merged grids: [n_iter][ncase][dim+2] max |res| (bits of a
+                                    // non-negative double, so integer max = numeric max)
 };
 
 struct Gas {

@@ -72,6 +72,9 @@ struct psst_grid {
     // initial state holder filled by psst_case_read (SoA p,T,u..)
     std::vector<double> prim0;
     double ref_vel = 0.0;
+    // merged grids (psst_grid_merge): volumes [case_vol_ptr[i], case_vol_ptr[i+1])
+    // belong to case i; empty for a single case
+    std::vector<int64_t> case_vol_ptr;
 };
 
 namespace psst {

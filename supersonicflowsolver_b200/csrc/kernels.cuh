@@ -329,6 +329,7 @@ __global__ void __launch_bounds__(256) k_face(DevGrid g, DevState<R> st, DevWork
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
     const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
+    if (g.cell_case && !g.case_active[g.cell_case[fr.c0]]) return;  // stopped case
     R nn[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) nn[k] = (R)fr.n[k];
@@ -389,6 +390,7 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
     constexpr int NVAR = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nint) return;
+    if (g.cell_case && !g.case_active[g.cell_case[c]]) return;  // stopped case
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
     const Prim<R, DIM> own = unpack<R, DIM>(ld16(st.rec + c));
@@ -410,7 +412,7 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
             const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
             const FaceRec<R, DIM> fr = ld16(frec + f);
-            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + (side ? fr.c0 : fr.c1)));
+            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + g.csr_nb[b + q]));
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -435,10 +437,8 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
         const R r0 = (R)g.lsq_r[c], r1 = (R)g.lsq_r[(int64_t)g.nint + c], r2 = (R)g.lsq_r[2 * (int64_t)g.nint + c];
         const R xc0 = (R)g.xc[c], xc1 = (R)g.xc[(int64_t)g.nall + c];
         for (int32_t j = 0; j < K; ++j) {
-            const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
-            const int32_t f = ent >> 1;
-            const FaceRec<R, DIM> fr = ld16(frec + f);
-            const int32_t nb = (ent & 1) ? fr.c0 : fr.c1;
+            const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
+            const int32_t nb = g.csr_nb[slot];
             const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + nb));
             if (CELLLIM)
 #pragma unroll
@@ -561,26 +561,40 @@ __device__ __forceinline__ double local_time(const DevGrid &g, const CellRec<R> 
     return (double)((R)cfl * (R)g.V[c] / den);
 }
 
+// Inputs of a cell's RK update: the previous-stage state (w on stage 0) and
+// the volume. Loaded by rk_load before the cell stores anything, so that the
+// loads issue together (stores to w/pw/dt could alias them).
+template <int NV>
+struct RkIn {
+    double pw[NV];
+    double vol;
+};
+
+template <typename R, int NV>
+__device__ __forceinline__ RkIn<NV> rk_load(const DevGrid &g, const DevWork<R> &wk, int first_stage, int32_t c) {
+    RkIn<NV> in;
+    const double *src = first_stage ? wk.w : wk.pw;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.pw[v] = src[(int64_t)v * g.nint + c];
+    in.vol = g.V[c];
+    return in;
+}
+
 // RK stage update of one cell given its residual (psstFiniteVolumeGrid.cpp:324-346):
 // w = prev_w - dt*a*res/V in FP64, primitives, norms; returns the new record.
 template <typename R, int DIM>
-__device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<R> &wk, const Gas &gas, double dt,
-                                                double alpha, int first_stage, int32_t c, const R res[DIM + 2],
-                                                double sq[DIM + 2], double mx[DIM + 2]) {
+__device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<R> &wk, const Gas &gas,
+                                                const RkIn<DIM + 2> &in, double dt, double alpha, int first_stage,
+                                                int32_t c, const R res[DIM + 2], double sq[DIM + 2],
+                                                double mx[DIM + 2]) {
     constexpr int NV = DIM + 2;
-    wk.dt[c] = dt;
-    const double vol = g.V[c];
+    const double vol = in.vol;
     double w[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const int64_t idx = (int64_t)v * g.nint + c;
-        double pw;
-        if (first_stage) {
-            pw = wk.w[idx];
-            wk.pw[idx] = pw;
-        } else {
-            pw = wk.pw[idx];
-        }
+        const double pw = in.pw[v];
+        if (first_stage) wk.pw[idx] = pw;
         w[v] = pw - dt * alpha * (double)res[v] / vol;
         wk.w[idx] = w[v];
         const double rv = (double)res[v];
@@ -601,6 +615,7 @@ __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<
     const double T = ((w[DIM + 1] / rho) - (vs * 0.5)) / gas.cv;
     const double p = rho * gas.rm * T;
     if (!(rho > 0.0 && T > 0.0)) flag_error(wk.err, ERR_BAD_STATE, c);
+    wk.dt[c] = dt;
     return pack<R, DIM>((R)p, (R)T, (R)rho, u);
 }
 
@@ -665,19 +680,21 @@ __device__ __forceinline__ void block_norm_partials(double sq[NV], double mx[NV]
     }
 }
 
-// Stage norms from the block partials (fixed-order strided sums + tree, so
-// reproducible), folded into the iteration's max over stages: the reference's
-// residual column is max over stages and cells of |res|
-// (psstFiniteVolumeGrid.cpp:331-332); the RMS column is this project's.
-// Executed by one whole block.
+// Stage norms from the block partials (fixed-order strided sums, warp shuffle
+// trees, then the warps in order: reproducible for a given block size), folded
+// into the iteration's max over stages: the reference's residual column is max
+// over stages and cells of |res| (psstFiniteVolumeGrid.cpp:331-332); the RMS
+// column is this project's. Executed by one whole block (a multiple of 32
+// threads).
 template <int NV>
 __device__ __forceinline__ void finish_norms(const double *part, int nblocks, int32_t nint, double *linf, double *l2,
                                              int it_slot) {
-    __shared__ double ss[NV][256], sm[NV][256];
-    const int t = threadIdx.x;
+    __shared__ double red[2 * NV][32];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     double s[NV], m[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) s[v] = m[v] = 0.0;
+#pragma unroll 4
     for (int b = t; b < nblocks; b += blockDim.x)
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -686,23 +703,27 @@ __device__ __forceinline__ void finish_norms(const double *part, int nblocks, in
         }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        ss[v][t] = s[v];
-        sm[v][t] = m[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s[v] += __shfl_down_sync(FULL, s[v], o);
+            m[v] = fmax(m[v], __shfl_down_sync(FULL, m[v], o));
+        }
+        if (lane == 0) {
+            red[v][wid] = s[v];
+            red[NV + v][wid] = m[v];
+        }
     }
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (t < w)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                ss[v][t] += ss[v][t + w];
-                sm[v][t] = fmax(sm[v][t], sm[v][t + w]);
-            }
-        __syncthreads();
-    }
     if (t < NV) {
-        const double r = sqrt(ss[t][0] / (double)(nint > 0 ? nint : 1));
+        double a = 0.0, x = 0.0;
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int i = 0; i < nw; ++i) {
+            a += red[t][i];
+            x = fmax(x, red[NV + t][i]);
+        }
+        const double r = sqrt(a / (double)(nint > 0 ? nint : 1));
         if (r > l2[it_slot * NV + t]) l2[it_slot * NV + t] = r;
-        if (linf[it_slot * NV + t] < sm[t][0]) linf[it_slot * NV + t] = sm[t][0];
+        if (linf[it_slot * NV + t] < x) linf[it_slot * NV + t] = x;
     }
 }
 
@@ -710,6 +731,32 @@ template <int NV>
 __global__ void __launch_bounds__(256) k_norm_finish(const double *part, int nblocks, int32_t nint, double *linf,
                                                      double *l2, int it_slot) {
     finish_norms<NV>(part, nblocks, nint, linf, l2, it_slot);
+}
+
+// Per-case max |res| on merged grids: cl[case][v] holds the bits of a
+// non-negative double, so an integer atomicMax is the numeric max (order-free,
+// hence deterministic). Lanes of one case (the usual warp: cases are
+// contiguous in device order) reduce first; cs < 0 contributes nothing. NaN
+// never enters (mx skips it, as the reference's `if (res < |r|)` does).
+// Called by all 32 lanes of every warp.
+template <int NV>
+__device__ __forceinline__ void case_max(unsigned long long *cl, int32_t cs, const double mx[NV]) {
+    const int32_t c0 = __shfl_sync(FULL, cs, 0);
+    if (__all_sync(FULL, cs == c0)) {
+        if (c0 < 0) return;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double m = mx[v];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            if ((threadIdx.x & 31) == 0 && m > 0.0)
+                atomicMax(cl + (int64_t)c0 * NV + v, (unsigned long long)__double_as_longlong(m));
+        }
+    } else if (cs >= 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            if (mx[v] > 0.0) atomicMax(cl + (int64_t)cs * NV + v, (unsigned long long)__double_as_longlong(mx[v]));
+    }
 }
 
 // The last block of a launch to finish reduces all partials (no extra launch).
@@ -753,8 +800,11 @@ __device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<
 // faces' terms in the cell's own face order (the reference's accumulation
 // order, psstLocalTimeCalculation.cpp:117-127, 189-203), RK update, the cell's
 // ghost cells, block norm partials; the last block finishes the stage norms.
+// At least 4 blocks of 256 per SM (64 registers): the pass is bound by the
+// latency of its gathers, and the occupancy gained outweighs a 24-byte spill
+// (0.61 -> 0.56 ms per launch on 6M tets, FP32).
 template <typename R, int DIM, int LC>
-__global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
+__global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
                                               double cfl, double dt_uniform, double alpha, int first_stage,
                                               int it_slot) {
     using FO = FaceOut<R, DIM>;
@@ -763,8 +813,21 @@ __global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevSta
     double sq[NV], mx[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
-    if (c < g.nint) {
+    int32_t cs = -1;  // case of this cell on merged grids (-1: none or stopped)
+    bool run = c < g.nint;
+    if (run && g.cell_case) {
+        cs = g.cell_case[c];
+        if (!g.case_active[cs]) {  // stopped case: carry the state over
+            cs = -1;
+            run = false;
+            st16(nxt.rec + c, ld16(cur.rec + c));
+            for (int32_t i = g.gptr[c]; i < g.gptr[c + 1]; ++i)
+                st16(nxt.rec + g.nint + i, ld16(cur.rec + g.nint + i));
+        }
+    }
+    if (run) {
         const FO *fo = reinterpret_cast<const FO *>(wk.fout);
+        const RkIn<NV> rin = rk_load<R, NV>(g, wk, first_stage, c);
         const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
         const uint64_t perm = g.wperm[c];
         // When the cell's own face order is the face-loop order (the usual
@@ -836,7 +899,7 @@ __global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevSta
             }
             dt = (double)((R)cfl * (R)g.V[c] / den);
         }
-        const CellRec<R> nrec = rk_update<R, DIM>(g, wk, gas, dt, alpha, first_stage, c, res, sq, mx);
+        const CellRec<R> nrec = rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, c, res, sq, mx);
         st16(nxt.rec + c, nrec);
         const int32_t g0 = g.gptr[c], g1 = g.gptr[c + 1];
         if (g1 > g0) {
@@ -847,6 +910,7 @@ __global__ void __launch_bounds__(256) k_cell(DevGrid g, DevState<R> cur, DevSta
             }
         }
     }
+    if (g.cell_case) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, cs, mx);
     block_norm_partials<NV>(sq, mx, wk.l2part);
     last_block_finish<NV>(wk.l2part, wk.ticket, g.nint, wk.linf, wk.l2, it_slot);
 }
@@ -860,6 +924,7 @@ __device__ __forceinline__ void update_from_buffers(const DevGrid &g, const DevS
                                                     double dt_uniform, double alpha, int first_stage, int32_t c,
                                                     double sq[DIM + 2], double mx[DIM + 2], bool seq) {
     constexpr int NV = DIM + 2;
+    const RkIn<NV> rin = rk_load<R, NV>(g, wk, first_stage, c);
     R res[NV];
     if (GATHER) {
         gather_residual<R, DIM>(g, reinterpret_cast<const FaceOut<R, DIM> *>(wk.fout), c, res);
@@ -873,7 +938,7 @@ __device__ __forceinline__ void update_from_buffers(const DevGrid &g, const DevS
         dt = local_time<R, DIM, 1, true>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
     else
         dt = local_time<R, DIM, LC, false>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
-    st16(nxt.rec + c, rk_update<R, DIM>(g, wk, gas, dt, alpha, first_stage, c, res, sq, mx));
+    st16(nxt.rec + c, rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, c, res, sq, mx));
 }
 
 template <typename R, int DIM, int LC, bool GATHER>

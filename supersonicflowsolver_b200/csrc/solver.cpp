@@ -12,14 +12,17 @@
 //    so every per-cell sum is formed in the reference's order whatever the
 //    device numbering, plus a 4-bit permutation that replays the cell's own
 //    face order (used by LocalAccTime1/2 and least squares).
-// One RK stage is one fused launch (k_stage: fluxes of each cell's faces,
-// in-order residual, local time step, RK update, the cell's ghosts, norms) in
-// the parallel modes, or face pass -> cell pass -> ghost pass -> norms for the
-// sequential LocalAccTime1 mode and the stage-by-stage API. Gradients run once
-// per iteration before stage 0 (psstFiniteVolumeGrid.cpp:307-308).
+// One RK stage is face pass -> cell pass (the cell pass also updates the
+// cell's ghosts and the norms) in the parallel modes, or face pass -> cell
+// update -> ghost pass -> norms for the sequential LocalAccTime1 mode and the
+// stage-by-stage API. Gradients run once per iteration before stage 0
+// (psstFiniteVolumeGrid.cpp:307-308).
+// Merged grids (psst_grid_merge) keep each case contiguous in device order and
+// carry a per-cell case id, per-case run flags and per-case residual columns.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -66,10 +69,11 @@ uint64_t hilbert_key(uint32_t *X, int b, int n) {
 }
 
 struct Layout {
-    int32_t nint = 0, nghost = 0, nall = 0, nface = 0, nfi = 0, nlevels = 0;
+    int32_t nint = 0, nghost = 0, nall = 0, nface = 0, nfi = 0, nlevels = 0, ncase = 1;
+    std::vector<int32_t> cell_case;   // merged grids: case of each device cell
     std::vector<int32_t> dev_of_vol;  // reference volume -> device cell (-1: inactive)
     std::vector<int64_t> vol_of_dev;  // device cell -> reference volume
-    std::vector<int32_t> c0, c1, csr_ptr, csr_ent, rank, gptr, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
+    std::vector<int32_t> c0, c1, csr_ptr, csr_ent, csr_nb, rank, gptr, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
     std::vector<uint64_t> wperm;
     std::vector<double> S, n, xf, beta, V, xc, lsq_r, vk_eps2, z_u, z_p, z_T;
 };
@@ -111,7 +115,19 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
             }
             key[i] = hilbert_key(X, bits, dim);
         }
-        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+        if (G.case_vol_ptr.empty()) {
+            std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+        } else {  // merged grid: each case stays contiguous, Hilbert order inside it
+            auto cs = [&](int64_t i) {
+                return std::upper_bound(G.case_vol_ptr.begin(), G.case_vol_ptr.end(), ref_int[i]) -
+                       G.case_vol_ptr.begin();
+            };
+            std::vector<int64_t> icase(L.nint);
+            for (int32_t i = 0; i < L.nint; ++i) icase[i] = cs(i);
+            std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+                return icase[a] != icase[b] ? icase[a] < icase[b] : key[a] < key[b];
+            });
+        }
     }
     L.vol_of_dev.assign(L.nall, -1);
     L.rank.assign(L.nint, 0);
@@ -137,6 +153,13 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         const int32_t d = L.nint + (int32_t)i;
         L.dev_of_vol[v] = d;
         L.vol_of_dev[d] = v;
+    }
+    if (!G.case_vol_ptr.empty()) {
+        L.ncase = (int32_t)G.case_vol_ptr.size() - 1;
+        L.cell_case.resize(L.nall);
+        for (int32_t d = 0; d < L.nall; ++d)
+            L.cell_case[d] = (int32_t)(std::upper_bound(G.case_vol_ptr.begin(), G.case_vol_ptr.end(),
+                                                        L.vol_of_dev[d]) - G.case_vol_ptr.begin()) - 1;
     }
     // faces: interior (both sides interior cells) first, then boundary
     std::vector<int64_t> fint, fbnd;
@@ -191,6 +214,7 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         L.csr_ptr[d + 1] = L.csr_ptr[d] + (int32_t)(G.vf_ptr[v + 1] - G.vf_ptr[v]);
     }
     L.csr_ent.resize(L.csr_ptr[L.nint]);
+    L.csr_nb.resize(L.csr_ptr[L.nint]);
     for (int32_t d = 0; d < L.nint; ++d) {
         const int64_t v = L.vol_of_dev[d];
         const int64_t b = G.vf_ptr[v], k = G.vf_ptr[v + 1] - b;
@@ -202,6 +226,7 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
             const int64_t f = G.vf_idx[b + idx[q]];
             const int side = G.f_c0[f] == v ? 0 : 1;
             L.csr_ent[L.csr_ptr[d] + q] = (dev_face[f] << 1) | side;
+            L.csr_nb[L.csr_ptr[d] + q] = side ? L.c0[dev_face[f]] : L.c1[dev_face[f]];
             pos[idx[q]] = q;
         }
         uint64_t perm = 0;
@@ -340,7 +365,18 @@ struct psst_solver {
     double dt_uniform = 0.0;
     int nblk = 1;  // blocks of the thread-per-cell kernels
     int norm_cap = 0;
+    int last_n = 0;                    // iterations of the last psst_explicit_solve
+    std::vector<int32_t> active_h;     // merged grids: per-case run flags (host copy)
+    // CUDA graphs of whole psst_explicit_solve calls, keyed by (n_iter, buffer parity)
+    bool use_graphs = false;
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, int>, int64_t> graph_launches;
 
+    void drop_graphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+        graph_launches.clear();
+    }
     void *dalloc_bytes(size_t n) {
         void *p = nullptr;
         ck(cudaMalloc(&p, std::max<size_t>(n, 16)), "cudaMalloc");
@@ -359,6 +395,7 @@ struct psst_solver {
     }
     ~psst_solver() {
         if (device >= 0) cudaSetDevice(device);
+        drop_graphs();
         for (void *p : allocs) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -422,16 +459,36 @@ void alloc_state(psst_solver *s, const psst_grid &G) {
     ck(cudaMemset(w.err, 0, 4 * sizeof(int32_t)), "memset");
 }
 
+// Residual-norm buffers for n_iter iterations (allocated once, grown on
+// demand; growing invalidates captured graphs, which hold the old pointers).
 template <typename R>
-void ensure_norms(psst_solver *s, int n_iter) {
+void reserve_norms(psst_solver *s, int n_iter) {
     DevWork<R> &w = work<R>(s);
     if (n_iter > s->norm_cap) {
+        s->drop_graphs();
         s->norm_cap = std::max(n_iter, 2 * s->norm_cap);
         w.linf = s->dalloc<double>((size_t)s->norm_cap * s->nv);
         w.l2 = s->dalloc<double>((size_t)s->norm_cap * s->nv);
+        if (s->L.ncase > 1)
+            w.case_linf = s->dalloc<unsigned long long>((size_t)s->norm_cap * s->L.ncase * s->nv);
     }
+}
+
+template <typename R>
+void zero_norms(psst_solver *s, int n_iter) {
+    DevWork<R> &w = work<R>(s);
     ck(cudaMemsetAsync(w.linf, 0, (size_t)n_iter * s->nv * sizeof(double), s->stream), "memset");
     ck(cudaMemsetAsync(w.l2, 0, (size_t)n_iter * s->nv * sizeof(double), s->stream), "memset");
+    if (w.case_linf)
+        ck(cudaMemsetAsync(w.case_linf, 0, (size_t)n_iter * s->L.ncase * s->nv * sizeof(unsigned long long),
+                           s->stream),
+           "memset");
+}
+
+template <typename R>
+void ensure_norms(psst_solver *s, int n_iter) {
+    reserve_norms<R>(s, n_iter);
+    zero_norms<R>(s, n_iter);
 }
 
 void check_err(psst_solver *s, const int32_t *err_dev) {
@@ -498,13 +555,44 @@ void iterations(psst_solver *s, int n_iter, Mark &&mark) {
     }
 }
 
+// n_iter iterations. With graphs on, the whole call (norm reset + every
+// launch) is captured once per (n_iter, buffer parity) and replayed.
 template <typename R>
 void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     DevWork<R> &w = work<R>(s);
-    ensure_norms<R>(s, n_iter);
-    ck(cudaEventRecord(s->ev0, s->stream), "event");
+    reserve_norms<R>(s, n_iter);
     int64_t launches = 0;
-    iterations<R>(s, n_iter, [&](int) { ++launches; });
+    ck(cudaEventRecord(s->ev0, s->stream), "event");
+    if (s->use_graphs) {
+        const std::pair<int, int> key(n_iter, s->cur);
+        auto it = s->graphs.find(key);
+        if (it == s->graphs.end()) {
+            ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+            cudaGraph_t gr = nullptr;
+            try {
+                zero_norms<R>(s, n_iter);
+                iterations<R>(s, n_iter, [&](int) { ++launches; });
+            } catch (...) {
+                cudaStreamEndCapture(s->stream, &gr);
+                if (gr) cudaGraphDestroy(gr);
+                throw;
+            }
+            ck(cudaStreamEndCapture(s->stream, &gr), "graph capture");
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            ck(e, "graph instantiate");
+            it = s->graphs.emplace(key, ex).first;
+            s->graph_launches[key] = launches;
+        } else {
+            launches = s->graph_launches[key];
+            if ((int64_t)n_iter * s->sc.rk_level % 2) s->cur ^= 1;
+        }
+        ck(cudaGraphLaunch(it->second, s->stream), "graph launch");
+    } else {
+        zero_norms<R>(s, n_iter);
+        iterations<R>(s, n_iter, [&](int) { ++launches; });
+    }
     ck(cudaEventRecord(s->ev1, s->stream), "event");
     ck(cudaGetLastError(), "kernel launch");
     std::vector<double> li((size_t)n_iter * s->nv), l2((size_t)n_iter * s->nv);
@@ -515,6 +603,7 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
     s->last_ms = ms;
     s->last_launches = launches;
+    s->last_n = n_iter;
     s->iter += n_iter;
     if (res_linf) std::memcpy(res_linf, li.data(), li.size() * sizeof(double));
     if (res_l2) std::memcpy(res_l2, l2.data(), l2.size() * sizeof(double));
@@ -607,6 +696,7 @@ void autotune(psst_solver *s, int n_iter, int *blocks) {
     }
     cudaFree(snap);
     s->iter = iter0;
+    s->drop_graphs();
     s->g.blk_grad = pick[0];
     s->g.blk_face = pick[1];
     s->g.blk_cell = pick[2];
@@ -782,6 +872,9 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     if (sc->order == 2 && sc->grad != 1 && G->dim != 2)
         raise(PSST_ERR_UNSUPPORTED, "least-squares gradient: the reference's 3D path writes out of bounds "
                                     "(psstGradCalculation.cpp:338); only 2D is supported");
+    if (sc->order == 2 && sc->grad != 1 && G->case_vol_ptr.size() > 2)
+        raise(PSST_ERR_UNSUPPORTED, "merged grids need Green-Gauss gradients (the least-squares table is "
+                                    "indexed across zones, psstGradCalculation.cpp:404-412)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         raise(PSST_ERR_CUDA, "no CUDA device available (libpsst_b200 has no CPU fallback)");
@@ -819,6 +912,7 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.xc = s->upload(L.xc);
     g.csr_ptr = s->upload(L.csr_ptr);
     g.csr_ent = s->upload(L.csr_ent);
+    g.csr_nb = s->upload(L.csr_nb);
     g.wperm = s->upload(L.wperm);
     g.lsq_r = s->upload(L.lsq_r);
     g.vk_eps2 = s->upload(L.vk_eps2);
@@ -836,6 +930,14 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.lvl_ptr = s->upload(L.lvl_ptr);
     g.nlevels = L.nlevels;
     g.blk_grad = g.blk_face = g.blk_cell = kBlock;
+    g.ncase = L.ncase;
+    if (L.ncase > 1) {
+        if (s->seq)
+            raise(PSST_ERR_UNSUPPORTED, "merged grids run LocalAccTime1 from stage-start values only (lc1_mode 1)");
+        g.cell_case = s->upload(L.cell_case);
+        s->active_h.assign(L.ncase, 1);
+        g.case_active = s->upload(s->active_h);
+    }
     if (sc->precision == 32)
         alloc_state<float>(s.get(), *G);
     else
@@ -903,6 +1005,7 @@ extern "C" psst_status psst_stage_update(psst_solver *s, int k, double *res_linf
     if (!s) raise(PSST_ERR_ARG, "null solver");
     if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
     if (k < 0 || k >= s->sc.rk_level) raise(PSST_ERR_ARG, "RK stage out of range");
+    if (s->L.ncase > 1) raise(PSST_ERR_UNSUPPORTED, "merged grids advance through psst_explicit_solve only");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     DISPATCH(s, stage_api)(s, k, res_linf);
     PSST_API_END
@@ -969,6 +1072,7 @@ extern "C" psst_status psst_solver_launch_shape(psst_solver *s, const int *set, 
         for (int i = 0; i < 3; ++i)
             if (set[i] != 0 && set[i] != 64 && set[i] != 128 && set[i] != 256)
                 raise(PSST_ERR_ARG, "launch shape must be 0 (keep), 64, 128 or 256 threads per block");
+        s->drop_graphs();
         if (set[0]) s->g.blk_grad = set[0];
         if (set[1]) s->g.blk_face = set[1];
         if (set[2]) s->g.blk_cell = set[2];
@@ -978,6 +1082,45 @@ extern "C" psst_status psst_solver_launch_shape(psst_solver *s, const int *set, 
         get[1] = s->g.blk_face;
         get[2] = s->g.blk_cell;
     }
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_use_graphs(psst_solver *s, int on) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    if (!on) s->drop_graphs();
+    s->use_graphs = on != 0;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_set_active(psst_solver *s, const int32_t *active) {
+    PSST_API_BEGIN
+    if (!s || !active) raise(PSST_ERR_ARG, "psst_solver_set_active: null argument");
+    if (s->L.ncase <= 1) raise(PSST_ERR_ARG, "psst_solver_set_active: the grid is not a merged grid");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    for (int32_t i = 0; i < s->L.ncase; ++i) s->active_h[i] = active[i] ? 1 : 0;
+    ck(cudaMemcpyAsync((void *)s->g.case_active, s->active_h.data(), s->active_h.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, s->stream),
+       "flags upload");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, double *out) {
+    PSST_API_BEGIN
+    if (!s || !out) raise(PSST_ERR_ARG, "psst_solver_case_residuals: null argument");
+    if (s->L.ncase <= 1) raise(PSST_ERR_ARG, "psst_solver_case_residuals: the grid is not a merged grid");
+    if (n_iter <= 0 || n_iter > s->last_n)
+        raise(PSST_ERR_ARG, "psst_solver_case_residuals: n_iter exceeds the last psst_explicit_solve call");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    const size_t cnt = (size_t)n_iter * s->L.ncase * s->nv;
+    std::vector<unsigned long long> h(cnt);
+    const unsigned long long *src = s->sc.precision == 32 ? s->w32.case_linf : s->w64.case_linf;
+    ck(cudaMemcpyAsync(h.data(), src, cnt * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->stream),
+       "norm copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    for (size_t i = 0; i < cnt; ++i) std::memcpy(out + i, &h[i], sizeof(double));
     PSST_API_END
 }
 

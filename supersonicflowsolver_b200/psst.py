@@ -121,6 +121,29 @@ class Grid:
                                          _ptr(prim)))
         return sc, prim
 
+    @classmethod
+    def merge(cls, grids):
+        """Disjoint union of case grids (each set up by read_case) for batched
+        solving; see psst_grid_merge."""
+        arr = (ctypes.c_void_p * len(grids))(*[g._h.value for g in grids])
+        h = ctypes.c_void_p()
+        check(_lib.load().psst_grid_merge(arr, len(grids), ctypes.byref(h)))
+        return cls(h)
+
+    def cases(self):
+        """Volume offsets of the cases (length ncase + 1)."""
+        n = ctypes.c_int32()
+        check(_lib.load().psst_grid_case_count(self._h, ctypes.byref(n), None))
+        ptr = np.zeros(n.value + 1, dtype=np.int64)
+        check(_lib.load().psst_grid_case_count(self._h, ctypes.byref(n), _ptr(ptr)))
+        return ptr
+
+    def initial_state(self):
+        """The state read by read_case (for a merged grid: all cases')."""
+        prim = np.zeros((2 + self.dim) * self.nvol)
+        check(_lib.load().psst_grid_initial_state(self._h, _ptr(prim), prim.size))
+        return prim
+
     def set_boundary(self, zone, dyn_id, u=None, p=0.0, therm_id=18, T=0.0):
         ua = np.zeros(3) if u is None else np.ascontiguousarray(u, dtype=np.float64)
         check(_lib.load().psst_grid_set_boundary(self._h, zone.encode(), dyn_id, _ptr(ua), p, therm_id, T))
@@ -212,6 +235,23 @@ class Solver:
         out = np.zeros(3, dtype=np.int32)
         check(_lib.load().psst_solver_launch_shape(self._h, _ptr(st), _ptr(out)))
         return dict(zip(("gradient", "face", "cell"), (int(x) for x in out)))
+
+    def use_graphs(self, on=True):
+        """Capture each explicit_solve call as a CUDA graph and replay it."""
+        check(_lib.load().psst_solver_use_graphs(self._h, int(bool(on))))
+
+    def set_active(self, flags):
+        """Merged grids: per-case run flags (stopped cases keep their state)."""
+        a = np.ascontiguousarray(np.asarray(flags, dtype=np.int32))
+        check(_lib.load().psst_solver_set_active(self._h, _ptr(a)))
+
+    def case_residuals(self, n_iter):
+        """Merged grids: per-case residual columns of the last explicit_solve,
+        shape (n_iter, ncase, dim+2)."""
+        ncase = len(self.grid.cases()) - 1
+        out = np.zeros((n_iter, ncase, self.nv))
+        check(_lib.load().psst_solver_case_residuals(self._h, int(n_iter), _ptr(out)))
+        return out
 
     def set_stream(self, stream_ptr):
         check(_lib.load().psst_solver_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
