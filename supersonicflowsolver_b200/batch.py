@@ -1,0 +1,120 @@
+"""Many ramp cases of uneven size and inflow solved together on one GPU.
+
+The cases' grids are merged into one (psst_grid_merge), so every kernel
+launch advances all of them; each iteration chunk is one CUDA-graph replay
+(psst_solver_use_graphs); launch shapes come from the solver's own tuner
+(psst_solver_autotune); per-case residual columns decide, case by case, when
+the residual drop is reached, and a converged case is stopped
+(psst_solver_set_active) so later launches skip its cells.
+
+Workload (seeded): mesh sizes uniform over {60x20, 120x40, 180x60, 240x80}
+quads (x by y), ramp angle U[5, 20] deg, Mach U[1.8, 4.0], p = 101325 Pa,
+T = 300 K; FP32, HLLC, cell-limited MUSCL, Green-Gauss, RK4, LocalAccTime1
+from stage-start values, CFL 0.5.
+
+    python -m supersonicflowsolver_b200.batch --cases 256 --seed 0
+"""
+import argparse
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import meshgen
+from .convergence import DropMonitor
+from .psst import Grid, Solver
+
+SIZES = [(60, 20), (120, 40), (180, 60), (240, 80)]
+
+
+def sample_cases(n, seed=0):
+    """n case descriptions: mesh size (nx, ny), ramp angle (deg), Mach."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = SIZES[int(rng.integers(len(SIZES)))]
+        out.append({"nx": nx, "ny": ny, "angle": float(rng.uniform(5.0, 20.0)), "mach": float(rng.uniform(1.8, 4.0))})
+    return out
+
+
+def build_cases(cases, directory, precision=32, flux=3, limiter=5, cfl=0.5, rk_level=4):
+    """Per-case grids set up from written case files; returns (grids, scheme)."""
+    grids, scheme = [], None
+    for i, c in enumerate(cases):
+        d = os.path.join(directory, "case%d" % i)
+        meshgen.write_case(d, "case", mach=c["mach"], max_iter=1, flux=flux, order=2, limiter=limiter, lc=1,
+                           cfl=cfl, rk_level=rk_level)
+        g = Grid.from_mesh(meshgen.wedge2d(c["nx"], c["ny"], c["angle"]))
+        sc, _ = g.read_case(d, "case")
+        sc.precision = precision
+        sc.lc1_mode = 1
+        sc.renumber = 1
+        grids.append(g)
+        scheme = sc
+    return grids, scheme
+
+
+def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100):
+    """Iterates all cases in chunks until every case reaches the residual drop
+    (or max_iter); cells[i] = interior cells of case i. Returns per-case
+    iterations to the drop, timings and the cell-iterations of running cases."""
+    ncase = len(cells)
+    mons = [DropMonitor(drop) for _ in range(ncase)]
+    active = np.ones(ncase, dtype=np.int32)
+    done, dev_s = 0, 0.0
+    cells_run = 0
+    t0 = time.perf_counter()
+    while done < max_iter and active.any():
+        n = min(chunk, max_iter - done)
+        solver.explicit_solve(n)
+        dev_s += solver.last_stats()[1] / 1000.0
+        cols = solver.case_residuals(n)
+        done += n
+        changed = False
+        for i in np.flatnonzero(active):
+            cells_run += int(cells[i]) * n
+            if mons[i].update(cols[:, i, :]):
+                active[i] = 0
+                changed = True
+        if changed and active.any():
+            solver.set_active(active)
+    wall = time.perf_counter() - t0
+    return {"iterations": [m.converged_at for m in mons], "run": done, "wall_s": wall, "device_s": dev_s,
+            "converged": int(sum(m.converged_at is not None for m in mons)), "cell_iterations": cells_run}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--cases", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--drop", type=float, default=1e-6)
+    ap.add_argument("--max-iter", type=int, default=50000)
+    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--limiter", type=int, default=5)
+    ap.add_argument("--precision", type=int, default=32)
+    a = ap.parse_args()
+    cases = sample_cases(a.cases, a.seed)
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        grids, sc = build_cases(cases, d, precision=a.precision, limiter=a.limiter)
+        merged = Grid.merge(grids)
+        solver = Solver(merged, sc)
+        solver.set_state(merged.initial_state())
+        setup_s = time.perf_counter() - t0
+        shapes = solver.autotune(2)
+        solver.use_graphs(True)
+        r = run_batch(solver, [g.ninterior for g in grids], drop=a.drop, max_iter=a.max_iter, chunk=a.chunk)
+    its = [x for x in r["iterations"] if x is not None]
+    out = {"cases": a.cases, "seed": a.seed, "cells": int(merged.ninterior), "setup_s": setup_s,
+           "threads_per_block": shapes, "converged": r["converged"], "iterations_run": r["run"],
+           "wall_s": r["wall_s"], "device_s": r["device_s"],
+           "cell_updates_per_s": r["cell_iterations"] / r["wall_s"],
+           "iterations_median": float(np.median(its)) if its else None,
+           "iterations_max": max(its) if its else None}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+"""Batched cases: merged grids (psst_grid_merge), per-case residual columns,
+per-case run flags and CUDA-graph replay.
+
+The merge is checked on the host; on the GPU every case of a merged grid must
+evolve bit for bit as it does alone (FP64), stopped cases must keep their
+state, and graph replays must equal plain launches.
+"""
+import numpy as np
+import pytest
+
+from supersonicflowsolver_b200 import meshgen
+from supersonicflowsolver_b200.psst import Grid, PsstError, Solver
+
+# (nx, ny, ramp angle, Mach): uneven sizes and inflows, as in the batch workload
+CASES = [(30, 10, 15.0, 2.5), (24, 8, 10.0, 3.0), (36, 12, 20.0, 2.0)]
+
+
+def build(tmp_path, precision=64, cases=CASES, **scheme):
+    kw = dict(flux=3, order=2, limiter=4, lc=1)
+    kw.update(scheme)
+    grids, schemes, prims = [], [], []
+    for i, (nx, ny, angle, mach) in enumerate(cases):
+        d = str(tmp_path / ("case%d" % i))
+        meshgen.write_case(d, "case", mach=mach, max_iter=1, **kw)
+        g = Grid.from_mesh(meshgen.wedge2d(nx, ny, angle))
+        sc, prim = g.read_case(d, "case")
+        sc.precision = precision
+        sc.lc1_mode = 1
+        grids.append(g)
+        schemes.append(sc)
+        prims.append(prim)
+    return grids, schemes, prims, Grid.merge(grids)
+
+
+def case_part(prim, merged, i, nvar):
+    """Case i's values of a merged prim array, in the case's own layout."""
+    ptr, nv = merged.cases(), merged.nvol
+    return np.concatenate([prim[q * nv + ptr[i]:q * nv + ptr[i + 1]] for q in range(nvar)])
+
+
+def test_merge_concatenates_cases(tmp_path):
+    grids, _, prims, m = build(tmp_path)
+    ptr = m.cases()
+    assert list(np.diff(ptr)) == [g.nvol for g in grids]
+    assert m.nvol == sum(g.nvol for g in grids) and m.nface == sum(g.nface for g in grids)
+    assert m.ninterior == sum(g.ninterior for g in grids)
+    assert np.array_equal(m.get("vol_V"), np.concatenate([g.get("vol_V") for g in grids]))
+    assert np.array_equal(m.get("face_n"), np.concatenate([g.get("face_n") for g in grids]))
+    assert np.array_equal(m.get("face_beta"), np.concatenate([g.get("face_beta") for g in grids]))
+    c0 = m.get("face_c0")
+    off = 0
+    f = 0
+    for g, base in zip(grids, ptr[:-1]):
+        gc0 = g.get("face_c0")
+        assert np.array_equal(c0[f:f + g.nface], np.where(gc0 < 0, -1, gc0 + base))
+        f += g.nface
+    prim = m.initial_state()
+    for i, p in enumerate(prims):
+        assert np.array_equal(case_part(prim, m, i, 4), p)
+    assert m.min_vol == min(g.min_vol for g in grids)
+    assert len(Grid.merge([grids[0]]).cases()) == 2
+
+
+def test_merge_rejects_mixed_dimensions(tmp_path):
+    g2 = Grid.from_mesh(meshgen.wedge2d(6, 3, 15.0))
+    g3 = Grid.from_mesh(meshgen.wedge3d(3, 2, 2, 12.0))
+    with pytest.raises(PsstError):
+        Grid.merge([g2, g3])
+
+
+@pytest.mark.gpu
+def test_merged_cases_evolve_as_alone(tmp_path):
+    grids, schemes, prims, m = build(tmp_path)
+    n = 6
+    solo = []
+    for g, sc, prim in zip(grids, schemes, prims):
+        s = Solver(g, sc)
+        s.set_state(prim)
+        linf, _ = s.explicit_solve(n)
+        solo.append((s.get_state(), linf))
+    b = Solver(m, schemes[0])
+    b.set_state(m.initial_state())
+    b.explicit_solve(n)
+    state, per_case = b.get_state(), b.case_residuals(n)
+    for i, (st, linf) in enumerate(solo):
+        assert np.array_equal(case_part(state, m, i, 4), st), "case %d state" % i
+        assert np.array_equal(per_case[:, i, :], linf), "case %d residual columns" % i
+
+
+@pytest.mark.gpu
+def test_stopped_case_keeps_its_state(tmp_path):
+    grids, schemes, prims, m = build(tmp_path)
+    b = Solver(m, schemes[0])
+    b.set_state(m.initial_state())
+    b.explicit_solve(2)
+    before = b.get_state()
+    b.set_active([1, 0, 1])
+    b.explicit_solve(3)
+    after = b.get_state()
+    per_case = b.case_residuals(3)
+    assert np.array_equal(case_part(after, m, 1, 4), case_part(before, m, 1, 4))
+    assert np.all(per_case[:, 1, :] == 0.0)
+    assert not np.array_equal(case_part(after, m, 0, 4), case_part(before, m, 0, 4))
+    # the running cases are unaffected by the stopped one
+    s = Solver(grids[2], schemes[2])
+    s.set_state(prims[2])
+    s.explicit_solve(5)
+    assert np.array_equal(case_part(after, m, 2, 4), s.get_state())
+    b.set_active([1, 1, 1])
+    linf, _ = b.explicit_solve(1)
+    assert np.all(b.case_residuals(1)[0, 1, :] > 0.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rk_level", [1, 4])
+def test_graph_replay_equals_plain_launches(tmp_path, rk_level):
+    """RK1 with 3 iterations per call flips the state buffers an odd number of
+    times per call, so replays alternate between the two captured parities."""
+    grids, schemes, prims, m = build(tmp_path, rk_level=rk_level)
+    runs = []
+    for graphs in (False, True):
+        b = Solver(m, schemes[0])
+        b.use_graphs(graphs)
+        b.set_state(m.initial_state())
+        cols = [b.explicit_solve(3)[0] for _ in range(4)]
+        runs.append((b.get_state(), np.concatenate(cols), b.case_residuals(3), b.iter))
+    for x, y in zip(runs[0], runs[1]):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_merged_grid_limits(tmp_path):
+    grids, schemes, prims, m = build(tmp_path)
+    sc = schemes[0]
+    sc.lc1_mode = 0
+    with pytest.raises(PsstError):
+        Solver(m, sc)
+    sc.lc1_mode = 1
+    b = Solver(m, sc)
+    b.set_state(m.initial_state())
+    with pytest.raises(PsstError):
+        b.stage_update(0)
+    s = Solver(grids[0], schemes[0])
+    with pytest.raises(PsstError):
+        s.set_active([1])
