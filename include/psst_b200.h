@@ -328,6 +328,41 @@ int64_t psst_solver_iter(const psst_solver *s);
 
 void psst_solver_destroy(psst_solver *s);
 
+/* ------------------------------------------------------------------------ */
+/* Learned warm start: coordinate MLP (no counterpart in the reference)      */
+/* ------------------------------------------------------------------------ */
+
+/* A 6-layer MLP of width 256 mapping (Mach, ramp angle, x, y), each normalised
+ * to [-1, 1], through 124 Fourier features (sin/cos(2^j pi v), j < 15, and v
+ * itself) to 4 outputs (normalised rho, u, v, p). Hidden layers use SiLU. The
+ * five hidden GEMMs of the forward and backward passes run on the tensor cores
+ * (tcgen05, BF16 operands, FP32 accumulation); master weights, gradients and
+ * Adam state are FP32. Input and target arrays are DEVICE pointers, row-major
+ * [B][4] FP32, on the network's device. */
+typedef struct psst_mlp psst_mlp;
+psst_status psst_mlp_create(int device, uint64_t seed, psst_mlp **out);
+int64_t psst_mlp_param_count(const psst_mlp *m);
+/* Parameters as one FP32 array: for each layer W [out][in] then b [out]. */
+psst_status psst_mlp_get_params(psst_mlp *m, float *out, int64_t n);
+psst_status psst_mlp_set_params(psst_mlp *m, const float *in, int64_t n); /* also resets Adam */
+psst_status psst_mlp_forward(psst_mlp *m, const float *x, int B, float *y);
+/* Loss (mean squared error over B x 4) and its gradient (host array, layout of
+ * psst_mlp_get_params) without changing the parameters. */
+psst_status psst_mlp_gradients(psst_mlp *m, const float *x, const float *t, int B, float *grads, float *loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) at learning rate lr; returns the loss
+ * before the step. */
+psst_status psst_mlp_train_step(psst_mlp *m, const float *x, const float *t, int B, float lr, float *loss);
+psst_status psst_mlp_set_stream(psst_mlp *m, void *stream);
+void psst_mlp_destroy(psst_mlp *m);
+
+/* The tensor-core GEMM on its own: D[z][m][n] = sum over k of split z of
+ * A[m][k] * B[n][k], BF16 device operands given by element strides
+ * (A[m][k] = A[m*a_sm + k*a_sk], B[n][k] = B[n*b_sn + k*b_sk]), FP32 device
+ * output with row stride d_sm, z over ceil(K / k_split) splits (plain element
+ * sum of the splits = the full product). Synchronises the stream. */
+psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn, int64_t b_sk,
+                              int M, int N, int K, int k_split, float *D, int64_t d_sm, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

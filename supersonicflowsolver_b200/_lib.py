@@ -26,6 +26,8 @@ EXPORTED = [
     "psst_solver_destroy", "psst_convective_residual_static",
     "psst_grid_merge", "psst_grid_case_count", "psst_grid_initial_state",
     "psst_solver_use_graphs", "psst_solver_set_active", "psst_solver_case_residuals",
+    "psst_mlp_create", "psst_mlp_param_count", "psst_mlp_get_params", "psst_mlp_set_params", "psst_mlp_forward",
+    "psst_mlp_gradients", "psst_mlp_train_step", "psst_mlp_set_stream", "psst_mlp_destroy", "psst_tc_gemm_bf16",
 ]
 
 
@@ -116,6 +118,16 @@ def load():
         "psst_solver_use_graphs": (I, [P, I]),
         "psst_solver_set_active": (I, [P, P]),
         "psst_solver_case_residuals": (I, [P, I, P]),
+        "psst_mlp_create": (I, [I, ctypes.c_uint64, ctypes.POINTER(P)]),
+        "psst_mlp_param_count": (I64, [P]),
+        "psst_mlp_get_params": (I, [P, P, I64]),
+        "psst_mlp_set_params": (I, [P, P, I64]),
+        "psst_mlp_forward": (I, [P, P, I, P]),
+        "psst_mlp_gradients": (I, [P, P, P, I, P, ctypes.POINTER(ctypes.c_float)]),
+        "psst_mlp_train_step": (I, [P, P, P, I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+        "psst_mlp_set_stream": (I, [P, P]),
+        "psst_mlp_destroy": (None, [P]),
+        "psst_tc_gemm_bf16": (I, [P, I64, I64, P, I64, I64, I, I, I, I, P, I64, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -92,13 +92,14 @@ def main():
     ap.add_argument("--drop", type=float, default=1e-6)
     ap.add_argument("--max-iter", type=int, default=50000)
     ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--flux", type=int, default=3, help="1 AUSM, 2 HLL, 3 HLLC")
     ap.add_argument("--limiter", type=int, default=5)
     ap.add_argument("--precision", type=int, default=32)
     a = ap.parse_args()
     cases = sample_cases(a.cases, a.seed)
     with tempfile.TemporaryDirectory() as d:
         t0 = time.perf_counter()
-        grids, sc = build_cases(cases, d, precision=a.precision, limiter=a.limiter)
+        grids, sc = build_cases(cases, d, precision=a.precision, flux=a.flux, limiter=a.limiter)
         merged = Grid.merge(grids)
         solver = Solver(merged, sc)
         solver.set_state(merged.initial_state())
@@ -107,7 +108,8 @@ def main():
         solver.use_graphs(True)
         r = run_batch(solver, [g.ninterior for g in grids], drop=a.drop, max_iter=a.max_iter, chunk=a.chunk)
     its = [x for x in r["iterations"] if x is not None]
-    out = {"cases": a.cases, "seed": a.seed, "cells": int(merged.ninterior), "setup_s": setup_s,
+    out = {"cases": a.cases, "seed": a.seed, "flux": a.flux, "limiter": a.limiter, "precision": a.precision,
+           "cells": int(merged.ninterior), "setup_s": setup_s,
            "threads_per_block": shapes, "converged": r["converged"], "iterations_run": r["run"],
            "wall_s": r["wall_s"], "device_s": r["device_s"],
            "cell_updates_per_s": r["cell_iterations"] / r["wall_s"],

@@ -112,7 +112,7 @@ def field_error(a, b, grid):
     return out
 
 
-def precision_study(nx, ny, angle=15.0, mach=2.5, fluxes=(2, 3, 1), limiter=4, jitter=0.15, seed=0,
+def precision_study(nx, ny, angle=15.0, mach=2.5, fluxes=(2, 3, 1), order=2, limiter=5, jitter=0.15, seed=0,
                     shuffle_seed=1, drop=1e-6, max_iter=100000, device=0):
     """FP64 and FP32 runs of each flux to the residual drop on one mesh; yields
     one result dict per flux with the FP32 field error against FP64."""
@@ -120,14 +120,15 @@ def precision_study(nx, ny, angle=15.0, mach=2.5, fluxes=(2, 3, 1), limiter=4, j
                            interior_first=shuffle_seed is not None)
     names = {1: "AUSM", 2: "HLL", 3: "HLLC"}
     for flux in fluxes:
-        res = {"mesh": "%dx%d quads" % (nx, ny), "jitter": jitter, "flux": names[flux], "limiter": limiter,
-               "angle": angle, "mach": mach, "drop": drop}
+        res = {"mesh": "%dx%d quads" % (nx, ny), "jitter": jitter, "flux": names[flux], "order": order,
+               "limiter": limiter if order == 2 else None, "angle": angle, "mach": mach, "drop": drop}
         states = {}
         for prec in (64, 32):
             with tempfile.TemporaryDirectory() as d:
-                grid, sc, prim = ramp2d_case(d, nx, ny, angle, mach, flux=flux, limiter=limiter, precision=prec,
-                                             mesh=mesh)
+                grid, sc, prim = ramp2d_case(d, nx, ny, angle, mach, flux=flux, order=order, limiter=limiter,
+                                             precision=prec, mesh=mesh)
                 s = Solver(grid, sc, device=device)
+                s.use_graphs(True)
                 s.set_state(prim)
                 r = run_to_drop(s, drop=drop, max_iter=max_iter)
                 states[prec] = s.get_state()
@@ -142,13 +143,16 @@ def main():
     ap.add_argument("study", choices=["jitter", "plain"])
     ap.add_argument("--nx", type=int, default=240)
     ap.add_argument("--ny", type=int, default=80)
-    ap.add_argument("--limiter", type=int, default=4)
+    ap.add_argument("--order", type=int, default=2)
+    ap.add_argument("--limiter", type=int, default=5)
+    ap.add_argument("--angle", type=float, default=15.0)
+    ap.add_argument("--mach", type=float, default=2.5)
     ap.add_argument("--drop", type=float, default=1e-6)
     ap.add_argument("--max-iter", type=int, default=100000)
     a = ap.parse_args()
     jitter, shuffle = (0.15, 1) if a.study == "jitter" else (0.0, None)
-    for r in precision_study(a.nx, a.ny, limiter=a.limiter, jitter=jitter, shuffle_seed=shuffle, drop=a.drop,
-                             max_iter=a.max_iter):
+    for r in precision_study(a.nx, a.ny, angle=a.angle, mach=a.mach, order=a.order, limiter=a.limiter, jitter=jitter,
+                             shuffle_seed=shuffle, drop=a.drop, max_iter=a.max_iter):
         print(json.dumps(r), flush=True)
 
 
