@@ -258,6 +258,25 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- GPU side ---
+def max_over_ranks(values, ws, device):
+    """Element-wise max over the ranks of the process group (the slowest
+    replica's times); identity for one rank."""
+    if ws <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def replica_throughput(ws, cells, steps, ms_max, e2e_s_max):
+    """Whole-job cell-updates/s of ws independent replicas of `cells` cells
+    run for `steps` iterations, timed by the slowest rank (device ms, e2e s)."""
+    return ws * cells * steps / (ms_max / 1000.0), ws * cells * steps / e2e_s_max
+
+
 def run_gpu(args):
     import torch
 
@@ -280,7 +299,7 @@ def run_gpu(args):
     solver.set_stream(stream.cuda_stream)
     solver.set_state(prim)
     nint = grid.ninterior
-    shapes = solver.autotune(2) if not args.no_autotune else solver.launch_shape()
+    shapes = solver.autotune(3) if not args.no_autotune else solver.launch_shape()
 
     def barrier():
         if ws > 1:
@@ -305,25 +324,18 @@ def run_gpu(args):
         launches, lib_ms = solver.last_stats()
         # end-to-end through the C ABI with host buffers
         host_prim = torch.from_numpy(prim).pin_memory()
+        host_out = torch.empty_like(host_prim).pin_memory()
         barrier()
         t0 = time.perf_counter()
         solver.set_state(host_prim.numpy())
         for _ in range(args.steps):
             solver.explicit_solve(1)
-        out = solver.get_state()
+        out = solver.get_state(out=host_out.numpy())
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     clocks = clk.summary()
-    ms_max = ms
-    e2e_max = e2e_s
-    if ws > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms, e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max, e2e_max = float(t[0]), float(t[1])
-    value = ws * nint * args.steps / (ms_max / 1000.0)
-    e2e_value = ws * nint * args.steps / e2e_max
+    ms_max, e2e_max = max_over_ranks([ms, e2e_s], ws, "cuda")
+    value, e2e_value = replica_throughput(ws, nint, args.steps, ms_max, e2e_max)
     # per-kernel timing for the roofline (CUDA events around each launch)
     prof = solver.profile(2)
     nnz = 2 * grid.nface - grid.nghost  # CSR entries: interior faces twice, boundary faces once
@@ -352,7 +364,7 @@ def run_gpu(args):
                     "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": (state_bytes / args.steps) + 2 * nv * 8 + 16,
                     "note": "set_state from pinned host memory + K psst_explicit_solve(1) calls each returning "
-                            "residual columns + get_state, all timed"},
+                            "residual columns + get_state into pinned host memory, all timed"},
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,

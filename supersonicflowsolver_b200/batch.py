@@ -56,12 +56,14 @@ def build_cases(cases, directory, precision=32, flux=3, limiter=5, cfl=0.5, rk_l
     return grids, scheme
 
 
-def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100):
+def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None):
     """Iterates all cases in chunks until every case reaches the residual drop
-    (or max_iter); cells[i] = interior cells of case i. Returns per-case
-    iterations to the drop, timings and the cell-iterations of running cases."""
+    (or max_iter); cells[i] = interior cells of case i; scales[i] (optional) a
+    fixed residual normalisation per case. Returns per-case iterations to the
+    drop, the normalisations used, timings and the cell-iterations of running
+    cases."""
     ncase = len(cells)
-    mons = [DropMonitor(drop) for _ in range(ncase)]
+    mons = [DropMonitor(drop, scale=None if scales is None else scales[i]) for i in range(ncase)]
     active = np.ones(ncase, dtype=np.int32)
     done, dev_s = 0, 0.0
     cells_run = 0
@@ -81,7 +83,8 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100):
         if changed and active.any():
             solver.set_active(active)
     wall = time.perf_counter() - t0
-    return {"iterations": [m.converged_at for m in mons], "run": done, "wall_s": wall, "device_s": dev_s,
+    return {"iterations": [m.converged_at for m in mons], "scales": [m.scale for m in mons], "run": done,
+            "wall_s": wall, "device_s": dev_s,
             "converged": int(sum(m.converged_at is not None for m in mons)), "cell_iterations": cells_run}
 
 

@@ -27,11 +27,13 @@ from .psst import Grid, Solver
 class DropMonitor:
     """Tracks the normalised residual columns of consecutive iterations."""
 
-    def __init__(self, drop=1e-6, scale_iters=5):
+    def __init__(self, drop=1e-6, scale_iters=5, scale=None):
+        """scale: a fixed normalisation (e.g. another run's iterations 1..5, so
+        that two starts of one case must reach the same absolute residual)."""
         self.drop = drop
-        self.scale_iters = scale_iters
+        self.scale_iters = 0 if scale is not None else scale_iters
         self.rows = 0
-        self.scale = None
+        self.scale = None if scale is None else np.asarray(scale, dtype=np.float64)
         self.converged_at = None
         self.last = None
 

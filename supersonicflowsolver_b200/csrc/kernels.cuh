@@ -1000,6 +1000,40 @@ __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevWork<R> wk) {
     for (int v = 0; v < DIM + 2; ++v) wk.res[(int64_t)v * g.nint + c] = res[v];
 }
 
+// Device cell records from / to the reference's volume-ordered SoA state
+// (p, T, u0.. per volume), so that host buffers move in one contiguous copy.
+template <typename R, int DIM>
+__global__ void k_gather_prim(int32_t nall, DevState<R> st, const double *prim, const int32_t *vol, int64_t nvol) {
+    const int32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nall) return;
+    const int64_t v = vol[d];
+    R u[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) u[k] = (R)prim[(2 + k) * nvol + v];
+    CellRec<R> r = pack<R, DIM>((R)prim[v], (R)prim[nvol + v], (R)0, u);
+    st16(st.rec + d, r);
+}
+
+template <typename R, int DIM>
+__global__ void k_scatter_prim(int32_t nall, DevState<R> st, double *prim, const int32_t *vol, int64_t nvol) {
+    const int32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nall) return;
+    const int64_t v = vol[d];
+    const CellRec<R> r = ld16(st.rec + d);
+    prim[v] = (double)r.v[RP];
+    prim[nvol + v] = (double)r.v[RT];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) prim[(2 + k) * nvol + v] = (double)r.v[RU + k];
+}
+
+template <typename R>
+__global__ void k_scatter_w(int32_t nint, int nv, const double *w, double *out, const int32_t *vol) {
+    const int32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nint) return;
+    const int64_t v = vol[d];
+    for (int q = 0; q < nv; ++q) out[v * nv + q] = w[(int64_t)q * nint + d];
+}
+
 // explicit_solve prologue (psstFiniteVolumeGrid.cpp:279-300): rho = p/(rm*T)
 // for every volume (initialize_field and load_boundary form it so), and w for
 // interior cells.

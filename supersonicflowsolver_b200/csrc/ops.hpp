@@ -21,6 +21,15 @@ struct Ops {
     static size_t face_out_bytes(int dim);
     static void prologue(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
                          cudaStream_t s);
+    // state <-> the reference's volume order on the device: prim is SoA
+    // p[nvol], T[nvol], u[dim][nvol] (FP64), vol[d] the volume of device cell d
+    static void gather_prim(int dim, const DevGrid &g, const DevState<R> &st, const double *prim,
+                            const int32_t *vol, int64_t nvol, cudaStream_t s);
+    static void scatter_prim(int dim, const DevGrid &g, const DevState<R> &st, double *prim, const int32_t *vol,
+                             int64_t nvol, cudaStream_t s);
+    // w[v][dim+2] per volume (interior cells only)
+    static void scatter_w(int dim, const DevGrid &g, const DevWork<R> &wk, double *w, const int32_t *vol,
+                          cudaStream_t s);
     // grad: 1 Green-Gauss, 2 least squares; celllim: 0, 4 (Barth-Jespersen), 5 (Venkatakrishnan)
     static void gradient(int dim, int grad, int celllim, const DevGrid &g, const DevState<R> &st,
                          const DevWork<R> &wk, cudaStream_t s);

@@ -29,6 +29,33 @@ void Ops<R>::prologue(int dim, const DevGrid &g, const DevState<R> &st, const De
         k_prologue<R, 3><<<nblocks(g.nall), kBlock, 0, s>>>(g, st, wk, gas);
 }
 
+template <typename R>
+void Ops<R>::gather_prim(int dim, const DevGrid &g, const DevState<R> &st, const double *prim, const int32_t *vol,
+                         int64_t nvol, cudaStream_t s) {
+    if (g.nall == 0) return;
+    if (dim == 2)
+        k_gather_prim<R, 2><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, st, prim, vol, nvol);
+    else
+        k_gather_prim<R, 3><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, st, prim, vol, nvol);
+}
+
+template <typename R>
+void Ops<R>::scatter_prim(int dim, const DevGrid &g, const DevState<R> &st, double *prim, const int32_t *vol,
+                          int64_t nvol, cudaStream_t s) {
+    if (g.nall == 0) return;
+    if (dim == 2)
+        k_scatter_prim<R, 2><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, st, prim, vol, nvol);
+    else
+        k_scatter_prim<R, 3><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, st, prim, vol, nvol);
+}
+
+template <typename R>
+void Ops<R>::scatter_w(int dim, const DevGrid &g, const DevWork<R> &wk, double *w, const int32_t *vol,
+                       cudaStream_t s) {
+    if (g.nint == 0) return;
+    k_scatter_w<R><<<nblocks(g.nint), kBlock, 0, s>>>(g.nint, dim + 2, wk.w, w, vol);
+}
+
 template <typename R, int DIM>
 static void gradient_dim(int grad, int celllim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
                          cudaStream_t s) {

@@ -366,6 +366,8 @@ struct psst_solver {
     int nblk = 1;  // blocks of the thread-per-cell kernels
     int norm_cap = 0;
     int last_n = 0;                    // iterations of the last psst_explicit_solve
+    int32_t *d_vol = nullptr;          // reference volume of each device cell
+    double *d_prim = nullptr, *d_w = nullptr;  // reference-ordered state staging
     std::vector<int32_t> active_h;     // merged grids: per-case run flags (host copy)
     // CUDA graphs of whole psst_explicit_solve calls, keyed by (n_iter, buffer parity)
     bool use_graphs = false;
@@ -640,9 +642,9 @@ void run_profile(psst_solver *s, int n_iter, double *ms, int64_t *cnt) {
     s->iter += n_iter;
 }
 
-// Launch-shape tuner: runs n_iter iterations per candidate block size on the
-// solver's own mesh and state, times each pass with events, keeps the fastest
-// shape per pass, and puts the state back (device-to-device snapshot of the
+// Launch-shape tuner: runs n_iter iterations per candidate block size (two
+// sweeps) on the solver's own mesh and state, times each pass with events,
+// keeps the fastest shape per pass, and puts the state back (device-to-device snapshot of the
 // primitive records and the conservative state; everything else a stage reads
 // is recomputed from those), so the solution and the iteration count are
 // unchanged. Results do not depend on the shapes except for the rounding of
@@ -668,7 +670,10 @@ void autotune(psst_solver *s, int n_iter, int *blocks) {
     int pick[3] = {s->g.blk_grad, s->g.blk_face, s->g.blk_cell};
     try {
         copy(true);
-        for (int b : cand) {
+        // two sweeps in opposite orders; each shape keeps its best time, so a
+        // transient (clock ramp, a neighbour's traffic) does not decide
+        for (int j = 0; j < 6; ++j) {
+            const int b = j < 3 ? cand[j] : cand[5 - j];
             s->g.blk_grad = s->g.blk_face = s->g.blk_cell = b;
             double ms[PSST_KERNEL_KINDS];
             int64_t cnt[PSST_KERNEL_KINDS];
@@ -704,61 +709,49 @@ void autotune(psst_solver *s, int n_iter, int *blocks) {
         for (int i = 0; i < 3; ++i) blocks[i] = pick[i];
 }
 
+// Device staging of the reference-ordered state: the host buffers move in one
+// contiguous copy each way (DMA straight from pinned memory when the caller's
+// buffer is pinned) and the permutation to and from the device layout runs on
+// the GPU.
+void ensure_staging(psst_solver *s) {
+    if (s->d_vol) return;
+    std::vector<int32_t> vol(s->L.nall);
+    for (int32_t d = 0; d < s->L.nall; ++d) vol[d] = (int32_t)s->L.vol_of_dev[d];
+    s->d_vol = s->upload(vol);
+    s->d_prim = s->dalloc<double>((size_t)(2 + s->dim) * s->nvol_ref);
+    s->d_w = s->dalloc<double>((size_t)s->nv * s->nvol_ref);
+}
+
 template <typename R>
 void set_state(psst_solver *s, const double *prim) {
-    const int dim = s->dim;
-    const int64_t nv = s->nvol_ref;
-    const int32_t nall = s->L.nall;
-    std::vector<CellRec<R>> h(nall);
-    for (int32_t d = 0; d < nall; ++d) {
-        const int64_t v = s->L.vol_of_dev[d];
-        CellRec<R> r;
-        std::memset(&r, 0, sizeof r);
-        r.v[RP] = (R)prim[v];
-        r.v[RT] = (R)prim[nv + v];
-        for (int k = 0; k < dim; ++k) r.v[RU + k] = (R)prim[(2 + k) * nv + v];
-        h[d] = r;
-    }
+    ensure_staging(s);
+    const size_t bytes = (size_t)(2 + s->dim) * s->nvol_ref * sizeof(double);
+    ck(cudaMemcpyAsync(s->d_prim, prim, bytes, cudaMemcpyHostToDevice, s->stream), "state upload");
     DevState<R> &st = states<R>(s)[s->cur];
-    ck(cudaMemcpyAsync(st.rec, h.data(), (size_t)nall * sizeof(CellRec<R>), cudaMemcpyHostToDevice, s->stream),
-       "state upload");
-    Ops<R>::prologue(dim, s->g, st, work<R>(s), s->gas, s->stream);
+    Ops<R>::gather_prim(s->dim, s->g, st, s->d_prim, s->d_vol, s->nvol_ref, s->stream);
+    Ops<R>::prologue(s->dim, s->g, st, work<R>(s), s->gas, s->stream);
     ck(cudaGetLastError(), "prologue");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
 }
 
 template <typename R>
 void get_state(psst_solver *s, double *prim, double *wout) {
-    const int dim = s->dim;
+    ensure_staging(s);
     const int64_t nv = s->nvol_ref;
-    const int32_t nall = s->L.nall, nint = s->L.nint;
-    std::vector<CellRec<R>> h(nall);
-    const DevState<R> &st = states<R>(s)[s->cur];
-    ck(cudaMemcpyAsync(h.data(), st.rec, (size_t)nall * sizeof(CellRec<R>), cudaMemcpyDeviceToHost, s->stream),
-       "state copy");
-    std::vector<double> hw;
-    if (wout) {
-        hw.resize((size_t)s->nv * nint);
-        ck(cudaMemcpyAsync(hw.data(), work<R>(s).w, hw.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
-           "state copy");
-    }
-    ck(cudaStreamSynchronize(s->stream), "stream sync");
     if (prim) {
-        std::fill(prim, prim + (size_t)(2 + dim) * nv, 0.0);
-        for (int32_t d = 0; d < nall; ++d) {
-            const int64_t v = s->L.vol_of_dev[d];
-            prim[v] = (double)h[d].v[RP];
-            prim[nv + v] = (double)h[d].v[RT];
-            for (int k = 0; k < dim; ++k) prim[(2 + k) * nv + v] = (double)h[d].v[RU + k];
-        }
+        const size_t bytes = (size_t)(2 + s->dim) * nv * sizeof(double);
+        ck(cudaMemsetAsync(s->d_prim, 0, bytes, s->stream), "memset");
+        Ops<R>::scatter_prim(s->dim, s->g, states<R>(s)[s->cur], s->d_prim, s->d_vol, nv, s->stream);
+        ck(cudaMemcpyAsync(prim, s->d_prim, bytes, cudaMemcpyDeviceToHost, s->stream), "state copy");
     }
     if (wout) {
-        std::fill(wout, wout + (size_t)s->nv * nv, 0.0);
-        for (int32_t d = 0; d < nint; ++d) {
-            const int64_t v = s->L.vol_of_dev[d];
-            for (int q = 0; q < s->nv; ++q) wout[(size_t)v * s->nv + q] = hw[(size_t)q * nint + d];
-        }
+        const size_t bytes = (size_t)s->nv * nv * sizeof(double);
+        ck(cudaMemsetAsync(s->d_w, 0, bytes, s->stream), "memset");
+        Ops<R>::scatter_w(s->dim, s->g, work<R>(s), s->d_w, s->d_vol, s->stream);
+        ck(cudaMemcpyAsync(wout, s->d_w, bytes, cudaMemcpyDeviceToHost, s->stream), "state copy");
     }
+    ck(cudaGetLastError(), "state scatter");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
 }
 
 template <typename R, int DIM>

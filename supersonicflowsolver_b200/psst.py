@@ -178,8 +178,12 @@ class Solver:
             raise ValueError("prim must hold (2+dim)*nvol values")
         check(_lib.load().psst_solver_set_state(self._h, _ptr(prim)))
 
-    def get_state(self, with_w=False):
-        prim = np.zeros((2 + self.dim) * self.grid.nvol)
+    def get_state(self, with_w=False, out=None):
+        """prim (and w) in the reference's volume order; `out` (optional, e.g.
+        a pinned buffer) receives prim."""
+        prim = out if out is not None else np.empty((2 + self.dim) * self.grid.nvol)
+        if prim.dtype != np.float64 or prim.size != (2 + self.dim) * self.grid.nvol or not prim.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of (2+dim)*nvol values")
         w = np.zeros(self.nv * self.grid.nvol) if with_w else None
         check(_lib.load().psst_solver_get_state(self._h, _ptr(prim), _ptr(w) if with_w else None))
         return (prim, w) if with_w else prim

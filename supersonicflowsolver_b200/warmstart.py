@@ -37,9 +37,11 @@ def freestream(mach):
     return rho, mach * math.sqrt(GAMMA * R_GAS * T_INF), P_INF
 
 
-def solve_batch(cases, precision, flux, limiter, max_iter, chunk, init=None, device=0):
+def solve_batch(cases, precision, flux, limiter, max_iter, chunk, init=None, scales=None, device=0):
     """Merged solve of `cases` from freestream, or from init(case_index, grid,
-    prim_of_case) -> prim_of_case. Returns per-case results and states."""
+    prim_of_case) -> prim_of_case; scales: per-case residual normalisations
+    (default: each run's own iterations 1..5). Returns per-case results and
+    states."""
     with tempfile.TemporaryDirectory() as d:
         grids, sc = bt.build_cases(cases, d, precision=precision, flux=flux, limiter=limiter)
     merged = Grid.merge(grids)
@@ -58,7 +60,7 @@ def solve_batch(cases, precision, flux, limiter, max_iter, chunk, init=None, dev
     s = Solver(merged, sc, device=device)
     s.set_state(prim)
     s.use_graphs(True)
-    r = bt.run_batch(s, [g.ninterior for g in grids], max_iter=max_iter, chunk=chunk)
+    r = bt.run_batch(s, [g.ninterior for g in grids], max_iter=max_iter, chunk=chunk, scales=scales)
     state = s.get_state()
     per_case = []
     for i, g in enumerate(grids):
@@ -89,9 +91,14 @@ def predict_prim(net, case, grid, prim):
     xy = grid.get("vol_x").reshape(nv, 2)[interior]
     x = torch.from_numpy(normalise_inputs(case["mach"], case["angle"], xy)).cuda()
     y = net.forward(x).cpu().numpy()
-    rho, u, v, p = fields_from_outputs(y, *freestream(case["mach"]))
-    rho = np.maximum(rho, 1e-3 * freestream(case["mach"])[0])
-    p = np.maximum(p, 1e-3 * P_INF)
+    rho_inf, speed, p_inf = freestream(case["mach"])
+    rho, u, v, p = fields_from_outputs(y, rho_inf, speed, p_inf)
+    # keep the start physical whatever the network says: the solver, not the
+    # network, decides when the case has converged
+    rho = np.clip(rho, 0.3 * rho_inf, 20.0 * rho_inf)
+    p = np.clip(p, 0.3 * p_inf, 40.0 * p_inf)
+    u = np.clip(u, -1.5 * speed, 1.5 * speed)
+    v = np.clip(v, -1.5 * speed, 1.5 * speed)
     out = prim.copy()
     out[:nv][interior] = p
     out[nv:2 * nv][interior] = p / (R_GAS * rho)
@@ -130,7 +137,7 @@ def main():
     ap.add_argument("--train-seeds", default="1-8")
     ap.add_argument("--test-seed", type=int, default=9)
     ap.add_argument("--cases", type=int, default=256)
-    ap.add_argument("--flux", type=int, default=1)
+    ap.add_argument("--flux", type=int, default=3)
     ap.add_argument("--limiter", type=int, default=5)
     ap.add_argument("--precision", type=int, default=64)
     ap.add_argument("--max-iter", type=int, default=20000)
@@ -139,11 +146,12 @@ def main():
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=None, help="write the trained parameters here (.npy)")
+    ap.add_argument("--params", default=None, help="skip data and training: load parameters (.npy)")
     a = ap.parse_args()
     lo, hi = (int(v) for v in a.train_seeds.split("-"))
     log = lambda m: print(m, flush=True)
     Xs, Ys, gen = [], [], []
-    for seed in range(lo, hi + 1):
+    for seed in ([] if a.params else range(lo, hi + 1)):
         cases = bt.sample_cases(a.cases, seed)
         r, grids, states = solve_batch(cases, a.precision, a.flux, a.limiter, a.max_iter, a.chunk)
         gen.append({"seed": seed, "converged": r["converged"], "wall_s": r["wall_s"]})
@@ -152,18 +160,28 @@ def main():
             x, y = samples(c, g, st)
             Xs.append(x)
             Ys.append(y)
-    X, Y = np.concatenate(Xs), np.concatenate(Ys)
     net = MLP(seed=0)
-    tr = train(net, X, Y, a.epochs, a.batch, a.lr, log=log)
+    if a.params:
+        net.set_params(np.load(a.params))
+        X, tr = np.zeros((0, 4)), {"epochs": 0, "steps": 0, "train_s": 0.0, "loss": [float("nan")]}
+    else:
+        X, Y = np.concatenate(Xs), np.concatenate(Ys)
+        tr = train(net, X, Y, a.epochs, a.batch, a.lr, log=log)
     if a.out:
         np.save(a.out, net.params())
     cases = bt.sample_cases(a.cases, a.test_seed)
     plain, grids, plain_states = solve_batch(cases, a.precision, a.flux, a.limiter, a.max_iter, a.chunk)
+    # the warm start must reach the same absolute residual as the freestream start
     warm, _, warm_states = solve_batch(cases, a.precision, a.flux, a.limiter, a.max_iter, a.chunk,
-                                       init=lambda i, g, pr: predict_prim(net, cases[i], g, pr))
+                                       init=lambda i, g, pr: predict_prim(net, cases[i], g, pr),
+                                       scales=plain["scales"])
     both = [i for i in range(a.cases) if plain["iterations"][i] and warm["iterations"][i]]
     ratio = [plain["iterations"][i] / warm["iterations"][i] for i in both]
     errs = [field_error(warm_states[i], plain_states[i], grids[i]) for i in both]
+    # the network's own error: its prediction against the plain converged field
+    pred = [field_error(predict_prim(net, cases[i], grids[i], plain_states[i]), plain_states[i], grids[i])
+            for i in both]
+    q = lambda v: [float(np.quantile(v, f)) for f in (0.1, 0.5, 0.9)] if len(v) else None
     out = {"train_points": int(len(X)), "generation": gen, "training": {k: tr[k] for k in ("epochs", "steps", "train_s")},
            "final_loss": tr["loss"][-1],
            "test": {"cases": a.cases, "both_converged": len(both),
@@ -175,6 +193,12 @@ def main():
                                               sum(warm["iterations"][i] for i in both)) if both else None,
                     "wall_plain_s": plain["wall_s"], "wall_warm_s": warm["wall_s"] + warm["init_s"],
                     "warm_inference_s": warm["init_s"],
+                    "iteration_ratio_q10_q50_q90": q(ratio),
+                    "cases_with_ratio_ge_3": int(sum(r >= 3.0 for r in ratio)),
+                    "prediction_rms_rel_q10_q50_q90": {k: q([e[k]["rms_rel"] for e in pred]) for k in ("rho", "p", "mach")},
+                    "converged_field_diff_rms_rel_q50_max": {k: [float(np.median([e[k]["rms_rel"] for e in errs])),
+                                                                 float(max(e[k]["rms_rel"] for e in errs))]
+                                                             for k in ("rho", "p", "mach")} if errs else None,
                     "converged_field_diff_max_rel": {k: max(e[k]["max_rel"] for e in errs) for k in ("rho", "p", "mach")}
                     if errs else None}}
     print(json.dumps(out), flush=True)
