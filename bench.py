@@ -135,14 +135,15 @@ def traffic_model(grid, nnz, kind):
     K = nnz / nint
     if kind == "face":
         # per face: face record read (64: c0,c1 (2i), S (g), n (3g), two FP32 offset vectors)
-        # and the face output record written (64: flux*area 5s, time-step terms 8s, padding);
+        # and the face output record written (48: flux*area 5s, time-step terms 7s);
         # per interior cell: state record (32) + gradient/limiter record (80); ghosts: state (32)
-        return nf * (64 + 64) + nint * (32 + 80) + ngh * 32
+        return nf * (64 + 48) + nint * (32 + 80) + ngh * 32
     if kind == "cell":
-        # per cell: CSR ptr (i) + K entries (i) + own-order perm (8) + V (g) + w, prev_w (FP64
-        # 2x5x8, a third more on stage 0 amortised) + new state record (32) + dt (g) + ghost ptr
-        # (i); per face: face output record (64); per ghost: record in and out (2x32) + ids (2i)
-        return nint * (4 + 4 * K + 8 + 8 + 90 + 32 + 8 + 4) + nf * 64 + ngh * 72
+        # per cell: CSR ptr (i) + K entries (i) + K face areas (s) + own-order perm (8) + V (g) +
+        # w, prev_w (FP64 2x5x8, a third more on stage 0 amortised) + new state record (32) + dt
+        # (g) + ghost ptr (i); per face: face output record (48); per ghost: record in and out
+        # (2x32) + ids (2i)
+        return nint * (4 + 4 * K + 4 * K + 8 + 8 + 90 + 32 + 8 + 4) + nf * 48 + ngh * 72
     if kind == "gradient":
         # per cell: CSR (i + K i) + perm + V + eps^2 + own state record (32) + gradient/limiter
         # record written (80); per face: face record (64) + beta (g); ghosts: state record (32)

@@ -115,6 +115,14 @@ psst_status psst_grid_get_array(const psst_grid *g, const char *name, void *out,
 
 void psst_grid_free(psst_grid *g);
 
+/* Writes <prefix>.cas and <prefix>.dat as psstAnsysOutputManager::output_data
+ * does (psstOutputManager.cpp:35-397): the mesh as read (vertices, faces with
+ * their file neighbours, cell types, zones) and p, T, rho, u.. of every
+ * volume zone. prim: state in the layout of psst_solver_get_state; rho[nvol]:
+ * densities (psst_solver_get_array "rho"). Grids built by psst_grid_merge
+ * carry no mesh and are rejected. */
+psst_status psst_write_fluent(const psst_grid *g, const double *prim, const double *rho, const char *prefix);
+
 /* No counterpart in the reference (it solves one case per process). Merges n
  * case grids, each already set up by psst_case_read, into one grid that is
  * their disjoint union, so that one solver advances all of them with every
@@ -226,7 +234,8 @@ psst_status psst_stage_update(psst_solver *s, int k, double *res_linf);
  * (max over stages and cells of |residual|) and RMS residuals. */
 psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *res_linf, double *res_l2);
 
-/* Debug/parity reads of device arrays, reference volume order:
+/* Reads of device arrays, reference volume order: "rho"[nvol] (density of
+ * every volume, ghosts included, as psst_write_fluent needs it),
  * "residual"[(dim+2)*nvol], "dt"[nvol], "grad_u"[nvol*dim*dim],
  * "grad_p"[nvol*dim], "grad_T"[nvol*dim], "limiter"[nvol*(dim+2)]. */
 psst_status psst_solver_get_array(psst_solver *s, const char *name, double *out, int64_t count);

@@ -24,7 +24,7 @@ EXPORTED = [
     "psst_solver_get_array", "psst_solver_set_stream", "psst_solver_last_stats", "psst_solver_profile",
     "psst_solver_autotune", "psst_solver_launch_shape", "psst_solver_iter",
     "psst_solver_destroy", "psst_convective_residual_static",
-    "psst_grid_merge", "psst_grid_case_count", "psst_grid_initial_state",
+    "psst_grid_merge", "psst_grid_case_count", "psst_grid_initial_state", "psst_write_fluent",
     "psst_solver_use_graphs", "psst_solver_set_active", "psst_solver_case_residuals",
     "psst_mlp_create", "psst_mlp_param_count", "psst_mlp_get_params", "psst_mlp_set_params", "psst_mlp_forward",
     "psst_mlp_gradients", "psst_mlp_train_step", "psst_mlp_set_stream", "psst_mlp_destroy", "psst_tc_gemm_bf16",
@@ -113,6 +113,7 @@ def load():
         "psst_solver_destroy": (None, [P]),
         "psst_convective_residual_static": (I, [ctypes.c_int32] * 5 + [P] * 7 + [D] * 4 + [P, P]),
         "psst_grid_merge": (I, [P, ctypes.c_int32, ctypes.POINTER(P)]),
+        "psst_write_fluent": (I, [P, P, P, S]),
         "psst_grid_case_count": (I, [P, P, P]),
         "psst_grid_initial_state": (I, [P, P, I64]),
         "psst_solver_use_graphs": (I, [P, I]),

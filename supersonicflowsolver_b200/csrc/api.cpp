@@ -41,7 +41,9 @@ extern "C" psst_status psst_grid_read_fluent(const char *path, psst_grid **out) 
     if (!path || !out) raise(PSST_ERR_ARG, "psst_grid_read_fluent: null argument");
     *out = nullptr;
     RawMesh m = read_fluent(path);
-    *out = build_grid(m);
+    psst_grid *g = build_grid(m);
+    g->raw = std::make_shared<RawMesh>(std::move(m));
+    *out = g;
     PSST_API_END
 }
 
@@ -91,7 +93,9 @@ extern "C" psst_status psst_grid_from_fluent(const psst_fluent_desc *d, psst_gri
             raise(PSST_ERR_ARG, "face zone range out of bounds");
         }
     }
-    *out = build_grid(m);
+    psst_grid *g = build_grid(m);
+    g->raw = std::make_shared<RawMesh>(std::move(m));
+    *out = g;
     PSST_API_END
 }
 

@@ -3,8 +3,9 @@
 // Like main.cpp:9-63 it reads ./problem_manager (mesh file name, case name),
 // the mesh and <case>.inp/.prop/.par|.sav/.bvp/.btq, then runs the iteration
 // loop on the GPU and writes <case>_residual.dat (iteration, seconds, residual
-// columns as psstFiniteVolumeGrid.cpp:369-396 prints them) and <case>.sav
-// (psstFiniteVolumeGrid.cpp:606-639) every iter_step iterations and at the end.
+// columns as psstFiniteVolumeGrid.cpp:369-396 prints them), <case>.sav
+// (psstFiniteVolumeGrid.cpp:606-639) and the Fluent <case>.cas/<case>.dat
+// (psstOutputManager.cpp) every iter_step iterations and at the end.
 // Options: --precision 32|64, --jacobi (LocalAccTime1 from stage-start
 // values), --no-renumber, --device N, --chunk N (iterations per launch batch).
 #include <chrono>
@@ -89,6 +90,7 @@ int main(int argc, char **argv) {
     psst_grid_get_array(g, "vol_zone", zone.data(), gi.nvol);
     psst_grid_get_array(g, "vol_boundary", bnd.data(), gi.nvol);
     const int nvv = gi.dim + 2;
+    std::vector<double> rho(gi.nvol);
     const std::string resname = std::string(cs) + "_residual.dat", savname = std::string(cs) + ".sav";
     FILE *rf = std::fopen(resname.c_str(), sc.iter == 1 ? "w" : "a");
     if (!rf) return die("residual file");
@@ -107,12 +109,16 @@ int main(int argc, char **argv) {
             std::fprintf(rf, "\n");
             if (sc.iter_step > 0 && it % sc.iter_step == 0) {
                 psst_solver_get_state(s, prim.data(), nullptr);
+                psst_solver_get_array(s, "rho", rho.data(), gi.nvol);
+                if (psst_write_fluent(g, prim.data(), rho.data(), cs)) return die("output");
                 write_sav(savname.c_str(), gi, prim, zone, bnd, it);
             }
         }
     }
     std::fclose(rf);
     psst_solver_get_state(s, prim.data(), nullptr);
+    psst_solver_get_array(s, "rho", rho.data(), gi.nvol);
+    if (psst_write_fluent(g, prim.data(), rho.data(), cs)) return die("output");
     write_sav(savname.c_str(), gi, prim, zone, bnd, psst_solver_iter(s));
     psst_solver_destroy(s);
     psst_grid_free(g);

@@ -39,13 +39,14 @@ struct alignas(16) FaceRec {
 
 // Output of the face pass for one face: flux * area (DIM+2), then the face's
 // local-time-step terms: for LocalAccTime1 the products u0.n and u1.n of the
-// two neighbours' velocities with the normal (DIM each), the mean sound speed
-// and the area; for LocalAccTime2 S |n_k| (DIM). Padded to 16 bytes.
+// two neighbours' velocities with the normal (DIM each) and the mean sound
+// speed (the face area comes from DevGrid::csr_s); for LocalAccTime2 S |n_k|
+// (DIM). 12 values: 48 bytes in FP32, 96 in FP64.
 template <typename R, int DIM>
 struct alignas(16) FaceOut {
     static constexpr int NV = DIM + 2;
-    static constexpr int Q0 = NV, Q1 = NV + DIM, CN = NV + 2 * DIM, SA = NV + 2 * DIM + 1;
-    R v[DIM == 3 ? 16 : 12];
+    static constexpr int Q0 = NV, Q1 = NV + DIM, CN = NV + 2 * DIM;
+    R v[12];
 };
 
 struct DevGrid {
@@ -61,6 +62,7 @@ struct DevGrid {
     const int32_t *csr_ptr;   // [nint+1]
     const int32_t *csr_ent;   // face << 1 | side, sorted by the reference's face-loop order
     const int32_t *csr_nb;    // the cell across each csr_ent face (saves a dependent load)
+    const void *csr_s;        // R per csr_ent: the face's area, rounded to R (LocalAccTime1)
     const uint64_t *wperm;    // [nint] 4-bit slots: k-th face of the cell's own face order
     const double *lsq_r;      // [3][nint] 2D least-squares coefficients (reference table)
     const double *vk_eps2;    // [nint] Venkatakrishnan epsilon^2 = (K h)^3, h = V^(1/dim)
@@ -82,6 +84,7 @@ struct DevGrid {
     // and the per-case run flag; cells of a stopped case keep their state
     int32_t ncase;
     const int32_t *cell_case;    // [nall]
+    const int32_t *face_case;    // [nface]
     const int32_t *case_active;  // [ncase]
 };
 

@@ -186,6 +186,7 @@ RawMesh read_fluent(const std::string &path) {
                 int64_t t = type;
                 if (type == 0 && !c.hex(t)) fmt("truncated cell section");
                 m.cell_zone.push_back(zid);
+                m.cell_type.push_back(t);
             }
         } else if (op == 13) {
             int64_t zid = h.number(16), first = h.number(16), last = h.number(16);

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -34,6 +35,7 @@ struct RawMesh {
     std::vector<int64_t> face_nodes;      // 1-based vertex ids
     std::vector<int64_t> face_c0, face_c1;  // 1-based file cell ids, 0 = none
     std::vector<int64_t> cell_zone;       // per file cell
+    std::vector<int64_t> cell_type;       // per file cell (Fluent type; empty when not given)
     std::vector<Zone> zones;              // file order (first appearance)
     int64_t zone_slot(int64_t id);        // find or append
 };
@@ -72,6 +74,9 @@ struct psst_grid {
     // initial state holder filled by psst_case_read (SoA p,T,u..)
     std::vector<double> prim0;
     double ref_vel = 0.0;
+    // the mesh as read (vertices, file faces, cell types, file zone ranges):
+    // what psst_write_fluent writes back; null for merged grids
+    std::shared_ptr<const psst::RawMesh> raw;
     // merged grids (psst_grid_merge): volumes [case_vol_ptr[i], case_vol_ptr[i+1])
     // belong to case i; empty for a single case
     std::vector<int64_t> case_vol_ptr;

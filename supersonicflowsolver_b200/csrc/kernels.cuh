@@ -323,13 +323,14 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
 //   reference adds the two sound speeds in the opposite order on the other
 //   side; IEEE addition is commutative) and S;
 //  LocalAccTime2 (:189-193): S |n_k|.
+// At most 72 registers: seven 128-thread blocks per SM (the tuned shape).
 template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
-__global__ void __launch_bounds__(256) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
+__global__ void __maxnreg__(72) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     using FO = FaceOut<R, DIM>;
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
+    if (g.face_case && !g.case_active[g.face_case[f]]) return;  // stopped case (merged grids)
     const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
-    if (g.cell_case && !g.case_active[g.cell_case[fr.c0]]) return;  // stopped case
     R nn[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) nn[k] = (R)fr.n[k];
@@ -366,7 +367,6 @@ __global__ void __launch_bounds__(256) k_face(DevGrid g, DevState<R> st, DevWork
             o.v[FO::Q1 + k] = p1.u[k] * nn[k];
         }
         o.v[FO::CN] = (sqrt(gr * p1.T) + sqrt(gr * p0.T)) * (R)0.5;
-        o.v[FO::SA] = S;
     } else if (LC == 2) {
 #pragma unroll
         for (int k = 0; k < DIM; ++k) o.v[FO::Q0 + k] = S * fabs(nn[k]);
@@ -407,8 +407,7 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
     for (int i = 0; i < NVAR; ++i) mx[i] = mn[i] = pvar<R, DIM>(own, i);
     if (GRAD == 1) {
         const double V = g.V[c];
-#pragma unroll 4
-        for (int32_t q = 0; q < K; ++q) {
+        for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
             const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
             const FaceRec<R, DIM> fr = ld16(frec + f);
@@ -474,7 +473,6 @@ __global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, Dev
     }
     if (CELLLIM) {
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
-#pragma unroll 4
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
             const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
@@ -803,7 +801,7 @@ __device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<
 // At least 4 blocks of 256 per SM (64 registers): the pass is bound by the
 // latency of its gathers, and the occupancy gained outweighs a 24-byte spill
 // (0.61 -> 0.56 ms per launch on 6M tets, FP32).
-template <typename R, int DIM, int LC>
+template <typename R, int DIM, int LC, bool BATCH>
 __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
                                               double cfl, double dt_uniform, double alpha, int first_stage,
                                               int it_slot) {
@@ -813,20 +811,15 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
     double sq[NV], mx[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
-    int32_t cs = -1;  // case of this cell on merged grids (-1: none or stopped)
     bool run = c < g.nint;
-    if (run && g.cell_case) {
-        cs = g.cell_case[c];
-        if (!g.case_active[cs]) {  // stopped case: carry the state over
-            cs = -1;
-            run = false;
-            st16(nxt.rec + c, ld16(cur.rec + c));
-            for (int32_t i = g.gptr[c]; i < g.gptr[c + 1]; ++i)
-                st16(nxt.rec + g.nint + i, ld16(cur.rec + g.nint + i));
-        }
+    if (BATCH && run && !g.case_active[g.cell_case[c]]) {  // stopped case: carry the state over
+        run = false;
+        st16(nxt.rec + c, ld16(cur.rec + c));
+        for (int32_t i = g.gptr[c]; i < g.gptr[c + 1]; ++i) st16(nxt.rec + g.nint + i, ld16(cur.rec + g.nint + i));
     }
     if (run) {
         const FO *fo = reinterpret_cast<const FO *>(wk.fout);
+        const R *csr_s = reinterpret_cast<const R *>(g.csr_s);
         const RkIn<NV> rin = rk_load<R, NV>(g, wk, first_stage, c);
         const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
         const uint64_t perm = g.wperm[c];
@@ -861,7 +854,7 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
                         nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];
                     }
                     nnb = (nnb + nv) * (R)0.5;
-                    den += (fabs(nnb) + o.v[FO::CN]) * o.v[FO::SA];
+                    den += (fabs(nnb) + o.v[FO::CN]) * csr_s[b + q];
                 } else if (LC == 2) {
 #pragma unroll
                     for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
@@ -872,7 +865,8 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
         if (LC != 0) {
             if (LC == 1 && !one_pass) {  // the cell's own face order differs: second pass
                 for (int32_t j = 0; j < K; ++j) {
-                    const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+                    const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
+                    const int32_t ent = g.csr_ent[slot];
                     const FO o = ld16(fo + (ent >> 1));
                     const int side = ent & 1;
                     R nv = (R)0;
@@ -882,7 +876,7 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
                         nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];  // neighbour u . n
                     }
                     nnb = (nnb + nv) * (R)0.5;
-                    den += (fabs(nnb) + o.v[FO::CN]) * o.v[FO::SA];
+                    den += (fabs(nnb) + o.v[FO::CN]) * csr_s[slot];
                 }
             } else if (LC == 2) {
                 if (!one_pass)
@@ -910,7 +904,7 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
             }
         }
     }
-    if (g.cell_case) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, cs, mx);
+    if (BATCH) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, run ? g.cell_case[c] : -1, mx);
     block_norm_partials<NV>(sq, mx, wk.l2part);
     last_block_finish<NV>(wk.l2part, wk.ticket, g.nint, wk.linf, wk.l2, it_slot);
 }

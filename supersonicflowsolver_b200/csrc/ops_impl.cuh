@@ -141,12 +141,21 @@ template <typename R, int DIM>
 static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const DevWork<R> &wk,
                    const Gas &gas, double cfl, double dtu, double alpha, int first, int it, cudaStream_t s) {
     const int bs = g.blk_cell, nb = nblocks(g.nint, bs);
+    if (g.cell_case) {  // merged grids: per-case run flags and residual columns
+        if (lc == 1)
+            k_cell<R, DIM, 1, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        else if (lc == 2)
+            k_cell<R, DIM, 2, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        else
+            k_cell<R, DIM, 0, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        return;
+    }
     if (lc == 1)
-        k_cell<R, DIM, 1><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 1, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
     else if (lc == 2)
-        k_cell<R, DIM, 2><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 2, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
     else
-        k_cell<R, DIM, 0><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 0, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
 }
 
 template <typename R>

@@ -436,6 +436,11 @@ void alloc_state(psst_solver *s, const psst_grid &G) {
         s->g.frec = s->upload(build_face_records<R, 2>(G, s->L, s->rec));
     else
         s->g.frec = s->upload(build_face_records<R, 3>(G, s->L, s->rec));
+    {  // face area per CSR entry, rounded to R as the face pass rounds it
+        std::vector<R> cs(s->L.csr_ent.size());
+        for (size_t q = 0; q < cs.size(); ++q) cs[q] = (R)s->L.S[s->L.csr_ent[q] >> 1];
+        s->g.csr_s = s->upload(cs);
+    }
     DevState<R> *st = states<R>(s);
     for (int b = 0; b < 2; ++b) {
         st[b].rec = s->dalloc<CellRec<R>>(nall);
@@ -471,7 +476,7 @@ void reserve_norms(psst_solver *s, int n_iter) {
         s->norm_cap = std::max(n_iter, 2 * s->norm_cap);
         w.linf = s->dalloc<double>((size_t)s->norm_cap * s->nv);
         w.l2 = s->dalloc<double>((size_t)s->norm_cap * s->nv);
-        if (s->L.ncase > 1)
+        if (!s->L.cell_case.empty())
             w.case_linf = s->dalloc<unsigned long long>((size_t)s->norm_cap * s->L.ncase * s->nv);
     }
 }
@@ -786,6 +791,16 @@ void get_array(psst_solver *s, const std::string &nm, double *out, int64_t count
         if (n != count) raise(PSST_ERR_ARG, nm + ": expected " + std::to_string(n) + " elements");
         std::fill(out, out + n, 0.0);
     };
+    if (nm == "rho") {  // density of every volume (ghosts included), as the state records hold it
+        need(nv);
+        std::vector<CellRec<R>> h(s->L.nall);
+        ck(cudaMemcpyAsync(h.data(), states<R>(s)[s->cur].rec, h.size() * sizeof(CellRec<R>), cudaMemcpyDeviceToHost,
+                           s->stream),
+           "copy");
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+        for (int32_t d = 0; d < s->L.nall; ++d) out[s->L.vol_of_dev[d]] = (double)h[d].v[RRHO];
+        return;
+    }
     if (nm == "dt") {
         need(nv);
         std::vector<double> h(nint);
@@ -924,10 +939,13 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.nlevels = L.nlevels;
     g.blk_grad = g.blk_face = g.blk_cell = kBlock;
     g.ncase = L.ncase;
-    if (L.ncase > 1) {
+    if (!L.cell_case.empty()) {
         if (s->seq)
             raise(PSST_ERR_UNSUPPORTED, "merged grids run LocalAccTime1 from stage-start values only (lc1_mode 1)");
         g.cell_case = s->upload(L.cell_case);
+        std::vector<int32_t> fc(L.nface);
+        for (int32_t f = 0; f < L.nface; ++f) fc[f] = L.cell_case[L.c0[f]];
+        g.face_case = s->upload(fc);
         s->active_h.assign(L.ncase, 1);
         g.case_active = s->upload(s->active_h);
     }
@@ -998,7 +1016,7 @@ extern "C" psst_status psst_stage_update(psst_solver *s, int k, double *res_linf
     if (!s) raise(PSST_ERR_ARG, "null solver");
     if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
     if (k < 0 || k >= s->sc.rk_level) raise(PSST_ERR_ARG, "RK stage out of range");
-    if (s->L.ncase > 1) raise(PSST_ERR_UNSUPPORTED, "merged grids advance through psst_explicit_solve only");
+    if (!s->L.cell_case.empty()) raise(PSST_ERR_UNSUPPORTED, "merged grids advance through psst_explicit_solve only");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     DISPATCH(s, stage_api)(s, k, res_linf);
     PSST_API_END
@@ -1090,7 +1108,7 @@ extern "C" psst_status psst_solver_use_graphs(psst_solver *s, int on) {
 extern "C" psst_status psst_solver_set_active(psst_solver *s, const int32_t *active) {
     PSST_API_BEGIN
     if (!s || !active) raise(PSST_ERR_ARG, "psst_solver_set_active: null argument");
-    if (s->L.ncase <= 1) raise(PSST_ERR_ARG, "psst_solver_set_active: the grid is not a merged grid");
+    if (s->L.cell_case.empty()) raise(PSST_ERR_ARG, "psst_solver_set_active: the grid is not a merged grid");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     for (int32_t i = 0; i < s->L.ncase; ++i) s->active_h[i] = active[i] ? 1 : 0;
     ck(cudaMemcpyAsync((void *)s->g.case_active, s->active_h.data(), s->active_h.size() * sizeof(int32_t),
@@ -1103,7 +1121,7 @@ extern "C" psst_status psst_solver_set_active(psst_solver *s, const int32_t *act
 extern "C" psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, double *out) {
     PSST_API_BEGIN
     if (!s || !out) raise(PSST_ERR_ARG, "psst_solver_case_residuals: null argument");
-    if (s->L.ncase <= 1) raise(PSST_ERR_ARG, "psst_solver_case_residuals: the grid is not a merged grid");
+    if (s->L.cell_case.empty()) raise(PSST_ERR_ARG, "psst_solver_case_residuals: the grid is not a merged grid");
     if (n_iter <= 0 || n_iter > s->last_n)
         raise(PSST_ERR_ARG, "psst_solver_case_residuals: n_iter exceeds the last psst_explicit_solve call");
     ck(cudaSetDevice(s->device), "cudaSetDevice");

@@ -144,6 +144,12 @@ class Grid:
         check(_lib.load().psst_grid_initial_state(self._h, _ptr(prim), prim.size))
         return prim
 
+    def write_fluent(self, prim, rho, prefix):
+        """<prefix>.cas and <prefix>.dat as PSST's output manager writes them."""
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        check(_lib.load().psst_write_fluent(self._h, _ptr(prim), _ptr(rho), str(prefix).encode()))
+
     def set_boundary(self, zone, dyn_id, u=None, p=0.0, therm_id=18, T=0.0):
         ua = np.zeros(3) if u is None else np.ascontiguousarray(u, dtype=np.float64)
         check(_lib.load().psst_grid_set_boundary(self._h, zone.encode(), dyn_id, _ptr(ua), p, therm_id, T))
@@ -206,7 +212,7 @@ class Solver:
         check(_lib.load().psst_explicit_solve(self._h, int(n_iter), _ptr(linf), _ptr(l2)))
         return linf, l2
 
-    _ARR = {"dt": 1, "residual": "nv", "limiter": "nv", "grad_u": "dd", "grad_p": "d", "grad_T": "d"}
+    _ARR = {"rho": 1, "dt": 1, "residual": "nv", "limiter": "nv", "grad_u": "dd", "grad_p": "d", "grad_T": "d"}
 
     def get(self, name):
         w = self._ARR[name]
@@ -316,8 +322,10 @@ class GridFV:
         self.solver.set_state(prim)
 
     def save_solution(self, path, iteration):
-        """Writes the .sav format of psstFiniteVolumeGrid.cpp:606-639."""
+        """Writes <case>.cas/<case>.dat (psstOutputManager.cpp) and the .sav
+        format of psstFiniteVolumeGrid.cpp:606-639 (psstGridFV::save_data)."""
         prim = self.solver.get_state()
+        self.grid.write_fluent(prim, self.solver.get("rho"), path[:-4] if path.endswith(".sav") else path)
         nv, dim = self.grid.nvol, self.grid.dim
         zone, bnd = self.grid.get("vol_zone"), self.grid.get("vol_boundary")
         with open(path, "w") as f:

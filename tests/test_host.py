@@ -156,3 +156,43 @@ def test_solver_without_gpu_fails_loudly(tmp_path):
     with pytest.raises(PsstError) as e:
         Solver(g, sc)
     assert e.value.status == 4
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE_DIR, "wedge.dat")), reason="reference sources absent")
+def test_fluent_writer_reproduces_shipped_case_and_data(tmp_path):
+    """psst_write_fluent on the shipped wedge case (state from the oracle, which
+    reproduces the shipped wedge.sav bit for bit) gives the shipped wedge.cas and
+    wedge.dat byte for byte (line ends aside: the shipped files are CRLF)."""
+    import shutil
+
+    from conftest import oracle_prim
+    from oracle.pyoracle import Oracle
+
+    for f in ("wedge.inp", "wedge.prop", "wedge.par", "wedge.bvp", "wedge.btq"):
+        shutil.copy(os.path.join(REFERENCE_DIR, f), tmp_path / f)
+    with open(os.path.join(REFERENCE_DIR, "wedge80_240.msh"), "rb") as src:
+        (tmp_path / "wedge80_240.msh").write_bytes(src.read().replace(b"\r", b""))
+    o = Oracle(str(tmp_path / "wedge80_240.msh"), str(tmp_path), "wedge")
+    o.run(3000)
+    g = Grid.read_fluent(str(tmp_path / "wedge80_240.msh"))
+    prim = oracle_prim(o, g.nvol, g.dim)
+    g.write_fluent(prim, o.get("vol_rho"), str(tmp_path / "out"))
+    for ext in ("cas", "dat"):
+        shipped = open(os.path.join(REFERENCE_DIR, "wedge." + ext), "rb").read().replace(b"\r", b"")
+        assert (tmp_path / ("out." + ext)).read_bytes() == shipped, ext
+
+
+def test_fluent_writer_round_trip(tmp_path):
+    """The written .cas reads back as the same grid (generated tet mesh, cell
+    types inferred from the faces)."""
+    m = meshgen.wedge3d(4, 3, 2, 12.0, tets=True)
+    g = Grid.from_mesh(m)
+    nv = g.nvol
+    prim = np.concatenate([np.full(nv, 101325.0), np.full(nv, 300.0), np.zeros(3 * nv)])
+    g.write_fluent(prim, np.full(nv, 1.1766), str(tmp_path / "t"))
+    g2 = Grid.read_fluent(str(tmp_path / "t.cas"))
+    assert (g2.nvol, g2.nface, g2.ninterior) == (g.nvol, g.nface, g.ninterior)
+    for a in ("vol_V", "face_S", "face_n", "vol_x"):
+        assert np.array_equal(g.get(a), g2.get(a)), a
+    txt = (tmp_path / "t.cas").read_text()
+    assert "(12 (2 1 " in txt and " 2 2 2" in txt  # tetrahedra (type 2)
