@@ -45,13 +45,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # name: (nx, ny, nz, mach, angle)
-    "wedge3d_6M_tets": (200, 100, 50, 3.0, 12.0),
-    "wedge3d_750k_tets": (100, 50, 25, 3.0, 12.0),  # small case for ncu captures
+    # the bandwidth benchmark: 200x100x50 hexes x 6 tets, FP32, MUSCL/Venkatakrishnan
+    "wedge3d_6M_tets": dict(dim=3, mesh=(200, 100, 50), mach=3.0, angle=12.0, precision=32, limiter=5,
+                            cpu_mesh=(40, 20, 4), cpu_procs=0),
+    # small case of the same workload for ncu captures
+    "wedge3d_750k_tets": dict(dim=3, mesh=(100, 50, 25), mach=3.0, angle=12.0, precision=32, limiter=5,
+                              cpu_mesh=(40, 20, 4), cpu_procs=0),
+    # the reference's own 2D case (40x120 quads, 15 deg, Mach 2.5), FP64, MUSCL/Barth-Jespersen; the CPU
+    # reference runs the same mesh on one core (it has no Barth-Jespersen: DM/VanLeer there)
+    "ramp2d_120x40_fp64": dict(dim=2, mesh=(120, 40), mach=2.5, angle=15.0, precision=64, limiter=4,
+                               cpu_mesh=(120, 40), cpu_procs=1),
 }
-SCHEME = dict(flux=3, order=2, limiter=5, grad=1, lc=1, rk_level=4, cfl=0.5)
-CPU_SAMPLE = (40, 20, 4)  # reduced mesh of the same workload for the CPU reference: 19,200 tets
-CPU_SAMPLE_SCHEME = dict(SCHEME, limiter=3)  # the reference has no Venkatakrishnan limiter: VanLeer/DM
+SCHEME = dict(flux=3, order=2, grad=1, lc=1, rk_level=4, cfl=0.5)
+CPU_LIMITER = 3  # the reference has no cell-based limiters: its DM/VanLeer path is timed
 
 
 def dist_env():
@@ -109,18 +115,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def ramp_mesh(dim, size, angle):
+    from supersonicflowsolver_b200 import meshgen
+
+    if dim == 2:
+        return meshgen.wedge2d(size[0], size[1], angle)
+    return meshgen.wedge3d(size[0], size[1], size[2], angle, tets=True)
+
+
 def build_case(workload, directory):
     from supersonicflowsolver_b200 import meshgen
     from supersonicflowsolver_b200.psst import Grid
 
-    nx, ny, nz, mach, angle = WORKLOADS[workload]
-    mesh = meshgen.wedge3d(nx, ny, nz, angle, tets=True)
+    w = WORKLOADS[workload]
+    mesh = ramp_mesh(w["dim"], w["mesh"], w["angle"])
     zones = [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
-    meshgen.write_case(directory, "bench", dim=3, zones=zones, mach=mach, max_iter=1, **SCHEME)
+    meshgen.write_case(directory, "bench", dim=w["dim"], zones=zones, mach=w["mach"], max_iter=1,
+                       limiter=w["limiter"], **SCHEME)
     grid = Grid.from_mesh(mesh)
     del mesh
     sc, prim = grid.read_case(directory, "bench")
-    sc.precision = 32
+    sc.precision = w["precision"]
     sc.lc1_mode = 1
     sc.renumber = 1
     return grid, sc, prim
@@ -184,7 +199,7 @@ def reference_binary():
     return port, "port"
 
 
-def cpu_run(n_iter, procs):
+def cpu_run(n_iter, procs, workload="wedge3d_6M_tets"):
     """Runs the reference (or the oracle port where the reference was not built)
     on the reduced mesh, `procs` independent processes, n_iter iterations each.
     Returns per-process per-iteration loop times (s) from the residual file's
@@ -192,10 +207,9 @@ def cpu_run(n_iter, procs):
     from supersonicflowsolver_b200 import meshgen
 
     exe, kind = reference_binary()
-    nx, ny, nz = CPU_SAMPLE
-    mach, angle = WORKLOADS["wedge3d_6M_tets"][3:5]
+    w = WORKLOADS[workload]
     base = tempfile.mkdtemp(prefix="psst_cpu_")
-    mesh = meshgen.wedge3d(nx, ny, nz, angle, tets=True)
+    mesh = ramp_mesh(w["dim"], w["cpu_mesh"], w["angle"])
     zones = [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
     meshgen.write_fluent(mesh, os.path.join(base, "m.msh"))
     runs = []
@@ -203,8 +217,8 @@ def cpu_run(n_iter, procs):
         d = os.path.join(base, "p%d" % p)
         os.makedirs(d)
         os.link(os.path.join(base, "m.msh"), os.path.join(d, "m.msh"))
-        meshgen.write_case(d, "c", dim=3, zones=zones, mach=mach, max_iter=n_iter, save_step=10 ** 6,
-                           **CPU_SAMPLE_SCHEME)
+        meshgen.write_case(d, "c", dim=w["dim"], zones=zones, mach=w["mach"], max_iter=n_iter, save_step=10 ** 6,
+                           limiter=CPU_LIMITER, **SCHEME)
         open(os.path.join(d, "problem_manager"), "w").write("m.msh\nc")
         runs.append(subprocess.Popen([exe], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
     for r in runs:
@@ -219,17 +233,28 @@ def cpu_run(n_iter, procs):
     return times, kind, mesh.ncells, exe
 
 
-def cpu_baseline(warm, steps, procs):
-    times, kind, ncells, exe = cpu_run(warm + steps, procs)
+def cpu_procs(workload):
+    n = WORKLOADS[workload]["cpu_procs"]
+    return n if n > 0 else max(1, os.cpu_count() or 1)
+
+
+def cpu_sample_text(workload, ncells):
+    w = WORKLOADS[workload]
+    mesh = "x".join(str(v) for v in w["cpu_mesh"])
+    kind = "tets (%s hexes x6" % mesh if w["dim"] == 3 else "quads (%s" % mesh
+    return "%d %s, same ramp/Mach/scheme, DM+VanLeer limiter)" % (ncells, kind)
+
+
+def cpu_baseline(warm, steps, workload):
+    times, kind, ncells, exe = cpu_run(warm + steps, cpu_procs(workload), workload)
     if not times:
         return None
     # the time column is cumulative ms-resolution wall time since the loop began
     span = [t[warm + steps - 1] - (t[warm - 1] if warm > 0 else 0.0) for t in times]
     rate = sum(ncells * steps / s for s in span if s > 0)
     return {"value": rate, "unit": "cell-updates/s", "cores": len(times), "kind": kind,
-            "sample": "%d tets (%dx%dx%d hexes x6, same ramp/Mach/scheme, DM+VanLeer limiter), "
-                      "%d timed + %d warm-up iterations per process, %d processes" %
-                      (ncells, *CPU_SAMPLE, steps, warm, len(times)),
+            "sample": "%s, %d timed + %d warm-up iterations per process, %d processes" %
+                      (cpu_sample_text(workload, ncells), steps, warm, len(times)),
             "binary": os.path.relpath(exe, ROOT)}
 
 
@@ -237,8 +262,7 @@ def run_reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    procs = max(1, os.cpu_count() or 1)
-    times, kind, ncells, exe = cpu_run(args.warmup + args.steps, procs)
+    times, kind, ncells, exe = cpu_run(args.warmup + args.steps, cpu_procs(args.workload), args.workload)
     if not times:
         print(json.dumps({"impl": "reference", "unavailable": "the reference binary produced no residual file"}))
         return
@@ -249,10 +273,12 @@ def run_reference_arm(args):
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "wedge3d_6M_tets (CPU sample %d tets)" % ncells, "scheme": "HLLC + DM/VanLeer, GG, RK4, "
-                   "LocalAccTime1, CFL 0.5, Mach 3, 12 deg", "parallelism": "%d independent processes" % len(times)},
+        "config": {"workload": "%s (CPU sample: %s)" % (args.workload, cpu_sample_text(args.workload, ncells)),
+                   "scheme": "HLLC + DM/VanLeer, GG, RK4, LocalAccTime1, CFL 0.5, Mach %g, %g deg" %
+                             (WORKLOADS[args.workload]["mach"], WORKLOADS[args.workload]["angle"]),
+                   "parallelism": "%d independent processes" % len(times)},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": len(times), "kind": kind,
-                         "sample": "%d tets per process, %d timed + %d warm-up iterations" %
+                         "sample": "%d cells per process, %d timed + %d warm-up iterations" %
                                    (ncells, args.steps, args.warmup)},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -301,6 +327,9 @@ def run_gpu(args):
     solver.set_state(prim)
     nint = grid.ninterior
     shapes = solver.autotune(3) if not args.no_autotune else solver.launch_shape()
+    wl = WORKLOADS[args.workload]
+    if wl["dim"] == 2:  # a small mesh: launch latency dominates, replay whole calls as graphs
+        solver.use_graphs(True)
 
     def barrier():
         if ws > 1:
@@ -352,15 +381,20 @@ def run_gpu(args):
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if wl["precision"] == 32 else "f64",
             "data": "synthetic",
             "config": {"workload": args.workload, "cells": nint, "faces": grid.nface,
-                       "scheme": "HLLC + MUSCL/Venkatakrishnan(K=5), Green-Gauss, RK4 std, LocalAccTime1 "
-                                 "(stage-start values), CFL 0.5, Mach 3, 12 deg ramp",
-                       "precision": "FP32 state/flux; FP64 geometry, RK state, residual norms",
+                       "scheme": "HLLC + MUSCL/%s, Green-Gauss, RK4 std, LocalAccTime1 (stage-start values), "
+                                 "CFL 0.5, Mach %g, %g deg ramp" %
+                                 ("Venkatakrishnan(K=5)" if wl["limiter"] == 5 else "Barth-Jespersen",
+                                  wl["mach"], wl["angle"]),
+                       "precision": ("FP32 state/flux; FP64 geometry, RK state, residual norms"
+                                     if wl["precision"] == 32 else "FP64 throughout (the parity path)"),
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "threads_per_block": shapes,
-                       "l2_flush": "not needed: >2.5 GB of mesh + state per step, L2 is 126 MB"},
+                       "l2_flush": ("not needed: >2.5 GB of mesh + state per step, L2 is 126 MB" if wl["dim"] == 3
+                                    else "none: this small case stays in L2 (not the bandwidth benchmark)")},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": (state_bytes / args.steps) + 2 * nv * 8 + 16,
@@ -377,7 +411,7 @@ def run_gpu(args):
             "finite": finite,
         }
         if not args.no_cpu_baseline:
-            cb = cpu_baseline(1, 10, max(1, os.cpu_count() or 1))
+            cb = cpu_baseline(1, 10 if wl["dim"] == 3 else 200, args.workload)
             line["cpu_baseline"] = cb
         print(json.dumps(line))
     solver.close()
