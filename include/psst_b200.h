@@ -110,7 +110,8 @@ psst_status psst_grid_get_info(const psst_grid *g, psst_grid_info *out);
 /* Copies a named array in reference order. Doubles: "vol_V", "vol_x"[nvol*dim],
  * "face_S", "face_n"[nface*dim], "face_x"[nface*dim], "face_beta". Int64:
  * "face_c0", "face_c1" (volume index, -1 none), "vol_zone", "vol_boundary",
- * "face_zone". count = element count of the out buffer. */
+ * "vol_bc" (zone type: 1 interior, 32 parent cell, else a ghost's boundary
+ * type), "face_zone". count = element count of the out buffer. */
 psst_status psst_grid_get_array(const psst_grid *g, const char *name, void *out, int64_t count);
 
 void psst_grid_free(psst_grid *g);

@@ -336,8 +336,30 @@ static int read_mesh(oracle_t *o, const char *path) {
             long zi = zone_add(o, zid);
             snprintf(o->z[zi].name, sizeof o->z[zi].name, "%s", name);
         } else if (op == 58 || op == 59) {
-            free(s.buf);
-            return fail(o, "mesh: cell/face trees (hanging nodes) are not supported by the oracle");
+            /* cell/face trees of adapted meshes (psstAnsysBuilder::read_cell_tree /
+             * read_face_tree, psstAnsysGridReader.cpp:1068-1116): parent/child
+             * links that no step of the loop reads; the parent zone gets bc 31
+             * if no section declared it (add_zones_storage_connection, :655-686) */
+            long first = parse_number(&lp, 16), last = parse_number(&lp, 16);
+            long parent = parse_number(&lp, 16);
+            (void)parse_number(&lp, 16);
+            maybe_skip_line(&lp, &s);
+            int known = 0;
+            for (long zi = 0; zi < o->nz; ++zi)
+                if (o->z[zi].id == parent) known = 1;
+            if (!known) {
+                long zi = zone_add(o, parent);
+                o->z[zi].first = first;
+                o->z[zi].last = last;
+                o->z[zi].bc = 31;
+                o->z[zi].size = last - first + 1;
+            }
+            for (long i = 0; i < last - first + 1; ++i) {
+                long nk, kid;
+                if (s_ulong(&s, &nk, 16)) return fail(o, "mesh: truncated tree section");
+                for (long j = 0; j < nk; ++j)
+                    if (s_ulong(&s, &kid, 16)) return fail(o, "mesh: truncated tree section");
+            }
         }
     }
     free(s.buf);

@@ -95,7 +95,7 @@ def run_to_drop(solver, drop=1e-6, max_iter=100000, chunk=200):
 def fields(prim, grid, gamma=1.4, R=287.0):
     """Interior density, pressure and Mach number from a prim array."""
     nv, dim = grid.nvol, grid.dim
-    interior = grid.get("vol_boundary") == 0
+    interior = grid.get("vol_bc") == 1
     p, T = prim[:nv], prim[nv:2 * nv]
     u = prim[2 * nv:].reshape(dim, nv)
     rho = p / (R * T)

@@ -147,6 +147,8 @@ extern "C" psst_status psst_grid_get_array(const psst_grid *g, const char *name,
         put_i(g->nvol, [&](int64_t i) { return g->vz[g->vol_vz[i]].id; });
     else if (nm == "vol_boundary")
         put_i(g->nvol, [&](int64_t i) { return (int64_t)g->vol_boundary[i]; });
+    else if (nm == "vol_bc")
+        put_i(g->nvol, [&](int64_t i) { return g->vz[g->vol_vz[i]].bc; });
     else
         raise(PSST_ERR_ARG, "unknown grid array " + nm);
     PSST_API_END

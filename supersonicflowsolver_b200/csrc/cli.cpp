@@ -23,17 +23,17 @@ static int die(const char *what) {
 }
 
 static bool write_sav(const char *path, const psst_grid_info &gi, const std::vector<double> &prim,
-                      const std::vector<int64_t> &zone, const std::vector<int64_t> &bnd, int64_t iter) {
+                      const std::vector<int64_t> &zone, const std::vector<int64_t> &vbc, int64_t iter) {
     FILE *f = std::fopen(path, "w");
     if (!f) return false;
     const int dim = gi.dim;
     const int64_t nv = gi.nvol;
     std::fprintf(f, "%lld\n", (long long)iter);
     int64_t v = 0;
-    while (v < nv) {  // interior zones in storage order, one block per zone
+    while (v < nv) {  // bc 1 zones in ascending id (private_save_solution, :606-639)
         int64_t e = v;
         while (e < nv && zone[e] == zone[v]) ++e;
-        if (!bnd[v]) {
+        if (vbc[v] == 1) {
             std::fprintf(f, "%lld\n%lld\n", (long long)zone[v], (long long)(e - v));
             for (int64_t i = v; i < e; ++i) {
                 std::fprintf(f, "%.11f %.11f ", prim[i], prim[nv + i]);
@@ -86,9 +86,9 @@ int main(int argc, char **argv) {
     psst_solver *s = nullptr;
     if (psst_solver_create(g, &sc, device, &s)) return die("solver");
     if (psst_solver_set_state(s, prim.data())) return die("state");
-    std::vector<int64_t> zone(gi.nvol), bnd(gi.nvol);
+    std::vector<int64_t> zone(gi.nvol), vbc(gi.nvol);
     psst_grid_get_array(g, "vol_zone", zone.data(), gi.nvol);
-    psst_grid_get_array(g, "vol_boundary", bnd.data(), gi.nvol);
+    psst_grid_get_array(g, "vol_bc", vbc.data(), gi.nvol);
     const int nvv = gi.dim + 2;
     std::vector<double> rho(gi.nvol);
     const std::string resname = std::string(cs) + "_residual.dat", savname = std::string(cs) + ".sav";
@@ -111,7 +111,7 @@ int main(int argc, char **argv) {
                 psst_solver_get_state(s, prim.data(), nullptr);
                 psst_solver_get_array(s, "rho", rho.data(), gi.nvol);
                 if (psst_write_fluent(g, prim.data(), rho.data(), cs)) return die("output");
-                write_sav(savname.c_str(), gi, prim, zone, bnd, it);
+                write_sav(savname.c_str(), gi, prim, zone, vbc, it);
             }
         }
     }
@@ -119,7 +119,7 @@ int main(int argc, char **argv) {
     psst_solver_get_state(s, prim.data(), nullptr);
     psst_solver_get_array(s, "rho", rho.data(), gi.nvol);
     if (psst_write_fluent(g, prim.data(), rho.data(), cs)) return die("output");
-    write_sav(savname.c_str(), gi, prim, zone, bnd, psst_solver_iter(s));
+    write_sav(savname.c_str(), gi, prim, zone, vbc, psst_solver_iter(s));
     psst_solver_destroy(s);
     psst_grid_free(g);
     return 0;

@@ -2,8 +2,7 @@
 //
 // Accepts the sections PSST's reader understands (psstAnsysDirector::build_step,
 // psstAnsysGridReader.cpp:1138-1306): 2 dimension, 10 vertices, 12 cells,
-// 13 faces, 39/45 zone names; 58/59 (cell/face trees of adapted meshes) are
-// rejected. Header fields are parsed the way private_parse_number does
+// 13 faces, 39/45 zone names, 58/59 cell/face trees of adapted meshes. Header fields are parsed the way private_parse_number does
 // (:1319-1374) and, like the reference, a header line that does not end with
 // '(' consumes the following line before the data are read. Unlike the
 // reference, CR characters are treated as whitespace, so CRLF files load.
@@ -228,7 +227,40 @@ RawMesh read_fluent(const std::string &path) {
             std::string name = h.name();
             m.zones[m.zone_slot(zid)].name = name;
         } else if (op == 58 || op == 59) {
-            raise(PSST_ERR_UNSUPPORTED, path + ": cell/face trees (hanging-node meshes) are not supported");
+            // cell/face trees of adapted meshes (read_cell_tree / read_face_tree,
+            // psstAnsysGridReader.cpp:1068-1116): kept for the case writer; no step
+            // of the loop reads them. A parent zone no section declared gets bc 31
+            // (add_zones_storage_connection, :655-686).
+            RawMesh::Tree t;
+            t.op = (int)op;
+            t.first = h.number(16);
+            t.last = h.number(16);
+            t.parent_zone = h.number(16);
+            t.child_zone = h.number(16);
+            if (!h.ends_with_paren()) {
+                const char *b, *e;
+                c.line(b, e);
+            }
+            bool known = false;
+            for (const Zone &z : m.zones) known = known || z.id == t.parent_zone;
+            if (!known) {
+                Zone &z = m.zones[m.zone_slot(t.parent_zone)];
+                z.first = t.first;
+                z.last = t.last;
+                z.bc = 31;
+                z.size = t.last - t.first + 1;
+            }
+            t.ptr.push_back(0);
+            for (int64_t i = 0; i < t.last - t.first + 1; ++i) {
+                int64_t nk, kid;
+                if (!c.hex(nk)) fmt("truncated tree section");
+                for (int64_t j = 0; j < nk; ++j) {
+                    if (!c.hex(kid)) fmt("truncated tree section");
+                    t.kids.push_back(kid);
+                }
+                t.ptr.push_back((int64_t)t.kids.size());
+            }
+            m.trees.push_back(std::move(t));
         }
     }
     if (m.dim != 2 && m.dim != 3) fmt("missing or invalid dimension section");

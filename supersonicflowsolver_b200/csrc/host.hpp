@@ -37,6 +37,12 @@ struct RawMesh {
     std::vector<int64_t> cell_zone;       // per file cell
     std::vector<int64_t> cell_type;       // per file cell (Fluent type; empty when not given)
     std::vector<Zone> zones;              // file order (first appearance)
+    struct Tree {                         // a 58 (cells) or 59 (faces) section
+        int op = 0;
+        int64_t first = 0, last = 0, parent_zone = 0, child_zone = 0;
+        std::vector<int64_t> ptr, kids;   // children of parent first + i: kids[ptr[i], ptr[i+1])
+    };
+    std::vector<Tree> trees;
     int64_t zone_slot(int64_t id);        // find or append
 };
 

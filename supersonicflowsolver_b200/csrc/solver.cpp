@@ -80,10 +80,9 @@ struct Layout {
 
 void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
     const int dim = G.dim;
-    for (auto &z : G.vz)
-        if (z.bc == 32) raise(PSST_ERR_UNSUPPORTED, "parent-cell zones (hanging-node meshes) are not supported");
-    for (auto &z : G.fz)
-        if (z.bc == 31) raise(PSST_ERR_UNSUPPORTED, "parent-face zones (hanging-node meshes) are not supported");
+    // Adapted meshes: parent cells (bc 32) are never updated and parent faces
+    // (bc 31) are in no cell's face list and in no face loop
+    // (psstAnsysGridReader.cpp:825-883), so neither has a device slot.
     if (G.max_faces > 16) raise(PSST_ERR_UNSUPPORTED, "cells with more than 16 faces are not supported");
     // interior cells in the reference's update order (psstFiniteVolumeGrid.cpp:312-318)
     std::vector<int64_t> ref_int;
@@ -164,8 +163,10 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
     // faces: interior (both sides interior cells) first, then boundary
     std::vector<int64_t> fint, fbnd;
     for (int64_t f = 0; f < G.nface; ++f) {
+        if (G.fz[G.f_fz[f]].bc == 31) continue;
         const int64_t a = G.f_c0[f], b = G.f_c1[f];
         if (a < 0 || b < 0) raise(PSST_ERR_FORMAT, "face without two neighbours");
+        if (L.dev_of_vol[a] < 0 || L.dev_of_vol[b] < 0) raise(PSST_ERR_FORMAT, "face next to a parent cell");
         const bool zone_interior = G.fz[G.f_fz[f]].bc == 2;
         const bool ga = G.vol_boundary[a], gb = G.vol_boundary[b];
         if (zone_interior && (ga || gb)) raise(PSST_ERR_FORMAT, "interior face next to a ghost cell");

@@ -1,8 +1,9 @@
 // Fluent case and data files of a solution, byte for byte as PSST's
 // psstAnsysOutputManager writes them (psstOutputManager.cpp:35-397): the .cas
 // repeats the mesh as read (vertices, faces with their file neighbours, cell
-// types, zones), the .dat holds p, T, rho, u, v (, w) per volume zone in
-// ascending zone id (ghost zones included; parent zones skipped).
+// types, the cell/face trees of adapted meshes, zones), the .dat holds p, T,
+// rho, u, v (, w) per volume zone in ascending zone id (ghost zones included;
+// parent-cell zones skipped).
 #include <cinttypes>
 #include <cstdio>
 #include <map>
@@ -68,12 +69,45 @@ void write_dat(const psst_grid &g, const double *prim, const double *rho, const 
     }
 }
 
+// One tree section per parent zone (private_write_cell_tree / _face_tree,
+// :266-351). Children hang off the parent entity whatever section listed them
+// (create_finite_volume_grid, psstAnsysGridReader.cpp:788-821); a zone's child
+// zone is the one the last section naming it as parent gave.
+void write_trees(FILE *f, const RawMesh &m, const std::map<int64_t, const Zone *> &zones, int op) {
+    const int64_t parent_bc = op == 58 ? 32 : 31;
+    std::map<int64_t, std::vector<int64_t>> kids;  // parent file index -> children
+    std::map<int64_t, int64_t> child_zone;
+    for (const RawMesh::Tree &t : m.trees) {
+        if (t.op != op) continue;
+        child_zone[t.parent_zone] = t.child_zone;
+        for (int64_t i = 0; i + 1 < (int64_t)t.ptr.size(); ++i) {
+            std::vector<int64_t> &k = kids[t.first + i];
+            k.insert(k.end(), t.kids.begin() + t.ptr[i], t.kids.begin() + t.ptr[i + 1]);
+        }
+    }
+    bool header = false;
+    for (auto &kv : zones) {
+        const Zone &z = *kv.second;
+        if (z.bc != parent_bc) continue;
+        if (!header) std::fprintf(f, op == 58 ? "(0 \"Cells Trees:\")\n" : "(0 \"Faces Trees:\")\n");
+        header = true;
+        auto cz = child_zone.find(z.id);
+        std::fprintf(f, "(%d (%" PRIx64 " %" PRIx64 " %" PRIx64 " %" PRIx64 ")(\n", op, z.first, z.last, z.id,
+                     cz == child_zone.end() ? (int64_t)0 : cz->second);
+        for (int64_t i = 0; i < z.size; ++i) {
+            auto it = kids.find(z.first + i);
+            const int64_t nk = it == kids.end() ? 0 : (int64_t)it->second.size();
+            std::fprintf(f, " %" PRIx64, nk);
+            for (int64_t j = 0; j < nk; ++j) std::fprintf(f, " %" PRIx64, it->second[j]);
+            std::fprintf(f, "\n");
+        }
+        std::fprintf(f, "))\n\n");
+    }
+}
+
 void write_cas(const psst_grid &g, const RawMesh &m, const std::string &path) {
     std::map<int64_t, const Zone *> zones;  // ascending id
     for (const Zone &z : m.zones) zones[z.id] = &z;
-    for (auto &kv : zones)
-        if (kv.second->bc == 31 || kv.second->bc == 32)
-            raise(PSST_ERR_UNSUPPORTED, "writing hanging-node meshes is not supported");
     File out(path, "cas");
     FILE *f = out.f;
     const int dim = m.dim;
@@ -91,7 +125,7 @@ void write_cas(const psst_grid &g, const RawMesh &m, const std::string &path) {
     std::fprintf(f, "(0 \"Faces:\")\n(13 (0 1 %" PRIx64 " 0))\n", nfile_faces);
     for (auto &kv : zones) {
         const Zone &z = *kv.second;
-        if (z.bc == 1) continue;  // face zones: interior, boundary (and parent) zones
+        if (z.bc == 1 || z.bc == 32) continue;  // face zones: interior, boundary and parent faces
         std::fprintf(f, "(13 (%" PRIx64 " %" PRIx64 " %" PRIx64 " %" PRIx64 " 0)(\n", z.id, z.first, z.last, z.bc);
         for (int64_t j = 0; j < z.size; ++j) {
             const int64_t loc = z.first + j - 1;
@@ -119,7 +153,7 @@ void write_cas(const psst_grid &g, const RawMesh &m, const std::string &path) {
     }
     for (auto &kv : zones) {
         const Zone &z = *kv.second;
-        if (z.bc != 1) continue;
+        if (z.bc != 1 && z.bc != 32) continue;
         std::fprintf(f, "(12 (%" PRIx64 " %" PRIx64 " %" PRIx64 " %" PRIx64 " 0)(\n", z.id, z.first, z.last, z.bc);
         for (int64_t i = 0; i < z.size; ++i) {
             if (i % 9 == 0 && i != 0) std::fprintf(f, "\n");
@@ -127,12 +161,14 @@ void write_cas(const psst_grid &g, const RawMesh &m, const std::string &path) {
         }
         std::fprintf(f, "\n))\n\n");
     }
+    write_trees(f, m, zones, 58);
+    write_trees(f, m, zones, 59);
     std::fprintf(f, "(0 \"Zones:\")\n");
     for (auto &kv : zones)
         if (kv.second->bc == 1)
             std::fprintf(f, "(39 (%" PRId64 " %s %s)())\n\n", kv.first, bc_name(1), kv.second->name.c_str());
     for (auto &kv : zones)
-        if (kv.second->bc != 1)
+        if (kv.second->bc != 1 && kv.second->bc != 31 && kv.second->bc != 32)
             std::fprintf(f, "(39 (%" PRId64 " %s %s)())\n\n", kv.first, bc_name(kv.second->bc), kv.second->name.c_str());
     (void)g;
 }

@@ -10,6 +10,11 @@ builds the same family of domains for any ramp angle and resolution:
 * ``wedge3d``: the 2D profile extruded in z, as hexahedra or split into six
   tetrahedra per hex along the main diagonal (Kuhn/Freudenthal split, which
   is conforming between neighbouring hexes);
+* ``refine2d`` / ``wedge2d_adapted``: one level of hanging-node refinement of
+  chosen quads, in the layout Fluent gives adapted meshes (the reference's
+  wedge_adaptation.msh): children in the fluid zone, parent cells in a
+  parent zone (bc 32), split faces kept in parent face zones (bc 31), and
+  the 58/59 cell and face trees;
 * ``write_fluent``: writes the mesh so that both the reference reader
   (psstAnsysDirector::build_step, psstAnsysGridReader.cpp:1138-1306) and this
   package's reader accept it.
@@ -30,6 +35,8 @@ import numpy as np
 ZONE_NAMES = {3: "symm", 4: "wedge", 5: "wall", 6: "out", 7: "up", 8: "in", 9: "side"}
 INTERIOR_ZONE = 10
 CELL_ZONE = 2
+PARENT_CELL_ZONE = 11
+PARENT_FACE_ZONE_OFFSET = 100  # parent faces of zone z live in zone z + 100
 
 
 @dataclasses.dataclass
@@ -47,8 +54,15 @@ class Mesh:
     dim: int
     verts: np.ndarray  # (nv, dim)
     cell_type: int  # Fluent cell type: 3 quad, 2 tet, 4 hex
-    ncells: int
+    ncells: int  # active cells (the fluid zone)
     face_zones: list  # list[FaceZone], in file order
+    # adapted meshes: parent cells (ids ncells .. ncells + nparents - 1, zone
+    # PARENT_CELL_ZONE) with their children (0-based active ids), and for each
+    # parent face zone (bc 31) its child zone and, per parent face, the local
+    # indices of its two halves in that child zone
+    nparents: int = 0
+    cell_children: np.ndarray = None  # (nparents, 4)
+    face_children: dict = dataclasses.field(default_factory=dict)  # parent zone id -> (child zone id, (n, 2))
 
     @property
     def nfaces(self):
@@ -162,6 +176,132 @@ def shuffle(mesh, seed):
     return Mesh(mesh.dim, mesh.verts, mesh.cell_type, mesh.ncells, newz)
 
 
+def refine2d(mesh, refine):
+    """One level of hanging-node refinement of the quads selected by the
+    boolean mask ``refine`` (ncells,): each becomes four children joined at its
+    centre, each face next to a refined cell is split at its midpoint. The
+    split face stays in the file as a parent face (bc 31, zone id + 100) with
+    its original neighbours; its halves replace it in its own zone, so a quad
+    next to a refined one has five faces (a hanging node). Active cells are
+    the unrefined cells in their order, then the children of each refined
+    cell; parents follow as zone PARENT_CELL_ZONE (bc 32)."""
+    assert mesh.dim == 2 and mesh.cell_type == 3 and mesh.nparents == 0
+    refine = np.asarray(refine, dtype=bool)
+    nc = mesh.ncells
+    # each cell's edges oriented with the cell on the left (c0 is left of n0->n1)
+    edges = [[] for _ in range(nc)]
+    for z in mesh.face_zones:
+        for i in range(len(z.c0)):
+            a, b = int(z.nodes[i, 0]), int(z.nodes[i, 1])
+            edges[z.c0[i]].append((a, b))
+            if z.c1[i] >= 0:
+                edges[z.c1[i]].append((b, a))
+    verts = [tuple(v) for v in mesh.verts]
+
+    def add_vert(x):
+        verts.append(tuple(x))
+        return len(verts) - 1
+
+    ref_ids = np.flatnonzero(refine)
+    unref = np.flatnonzero(~refine)
+    new_id = np.full(nc, -1, dtype=np.int64)
+    new_id[unref] = np.arange(len(unref))
+    corners, child_of = {}, {}  # refined cell -> CCW corners; -> 4 child ids
+    for r, c in enumerate(ref_ids):
+        nxt = {a: b for a, b in edges[c]}
+        assert len(nxt) == 4, "refine2d needs plain quads"
+        v = [edges[c][0][0]]
+        for _ in range(3):
+            v.append(nxt[v[-1]])
+        corners[c] = v
+        child_of[c] = len(unref) + 4 * r + np.arange(4)
+    mid = {}  # undirected edge -> midpoint vertex
+
+    def midpoint(a, b):
+        k = (min(a, b), max(a, b))
+        if k not in mid:
+            mid[k] = add_vert(0.5 * (np.asarray(verts[a]) + np.asarray(verts[b])))
+        return mid[k]
+
+    def half_cell(c, a, b, first):
+        """Active cell on the left of the half of edge a->b (cell c on its left)
+        that touches a (first) or b."""
+        if not refine[c]:
+            return new_id[c]
+        v = corners[c]
+        k = v.index(a)
+        return child_of[c][k] if first else child_of[c][(k + 1) % 4]
+
+    pid = np.full(nc, -1, dtype=np.int64)
+    ntot_active = len(unref) + 4 * len(ref_ids)
+    pid[ref_ids] = ntot_active + np.arange(len(ref_ids))
+
+    def cell_ref(c):  # a cell as a parent face's neighbour
+        return pid[c] if refine[c] else new_id[c]
+
+    zones, parents = [], []
+    for z in mesh.face_zones:
+        nodes, c0, c1 = [], [], []
+        pn, p0, p1, kids = [], [], [], []
+        for i in range(len(z.c0)):
+            a, b = int(z.nodes[i, 0]), int(z.nodes[i, 1])
+            l, r = int(z.c0[i]), int(z.c1[i])
+            if not (refine[l] or (r >= 0 and refine[r])):
+                nodes.append((a, b))
+                c0.append(new_id[l])
+                c1.append(new_id[r] if r >= 0 else -1)
+                continue
+            m = midpoint(a, b)
+            pn.append((a, b))
+            p0.append(cell_ref(l))
+            p1.append(cell_ref(r) if r >= 0 else -1)
+            kids.append((len(nodes), len(nodes) + 1))
+            for (s, e), first in (((a, m), True), ((m, b), False)):
+                nodes.append((s, e))
+                c0.append(half_cell(l, a, b, first))
+                c1.append(half_cell(r, b, a, not first) if r >= 0 else -1)
+        if z.zone_id == INTERIOR_ZONE:
+            for c in ref_ids:
+                v = corners[c]
+                ctr = add_vert(np.mean([verts[q] for q in v], axis=0))
+                ms = [midpoint(v[k], v[(k + 1) % 4]) for k in range(4)]
+                for k in range(4):  # child k left of m_k -> centre, child k+1 right of it
+                    nodes.append((ms[k], ctr))
+                    c0.append(child_of[c][k])
+                    c1.append(child_of[c][(k + 1) % 4])
+        zones.append(FaceZone(z.zone_id, z.bc_type, z.name, np.asarray(nodes, dtype=np.int64).reshape(-1, 2),
+                              np.asarray(c0, dtype=np.int64), np.asarray(c1, dtype=np.int64)))
+        if pn:
+            parents.append((FaceZone(z.zone_id + PARENT_FACE_ZONE_OFFSET, 31, "", np.asarray(pn, dtype=np.int64),
+                                     np.asarray(p0, dtype=np.int64), np.asarray(p1, dtype=np.int64)),
+                            z.zone_id, np.asarray(kids, dtype=np.int64)))
+    face_children = {pz.zone_id: (cz, k) for pz, cz, k in parents}
+    cell_children = np.stack([child_of[c] for c in ref_ids]) if len(ref_ids) else np.zeros((0, 4), np.int64)
+    return Mesh(2, np.asarray(verts, dtype=np.float64), 3, ntot_active, zones + [p[0] for p in parents],
+                len(ref_ids), cell_children, face_children)
+
+
+def wedge2d_adapted(nx=40, ny=12, angle_deg=15.0, refine_frac=0.25, seed=0, **kw):
+    """wedge2d with a seeded random fraction of its quads refined once, plus
+    every quad in the band x in [0.4, 1.2] next to the ramp foot and the
+    oblique shock (where an adaptation would put cells)."""
+    base = wedge2d(nx, ny, angle_deg, **kw)
+    rng = np.random.default_rng(seed)
+    refine = rng.random(base.ncells) < refine_frac
+    xc = np.zeros(base.ncells)
+    cnt = np.zeros(base.ncells)
+    for z in base.face_zones:
+        xm = base.verts[z.nodes].mean(axis=1)[:, 0]
+        np.add.at(xc, z.c0, xm)
+        np.add.at(cnt, z.c0, 1)
+        inner = z.c1 >= 0
+        np.add.at(xc, z.c1[inner], xm[inner])
+        np.add.at(cnt, z.c1[inner], 1)
+    xc /= cnt
+    refine |= (xc > 0.4) & (xc < 1.2)
+    return refine2d(base, refine)
+
+
 def wedge3d(nx=200, ny=100, nz=50, angle_deg=12.0, length=3.0, height=1.0, depth=1.0, ramp_x0=0.5,
             ramp_top=0.2, tets=True, interior_first=False):
     """The 2D profile extruded over z in [0, depth]: hexahedra or 6 Kuhn tets per hex."""
@@ -271,11 +411,31 @@ def write_fluent(mesh, path):
             np.savetxt(f, cols, fmt="%x")
             f.write("))\n")
             first += n
-        f.write("\n(12 (0 1 %x 0))\n" % mesh.ncells)
+        zfirst, first = {}, 1
+        for z in mesh.face_zones:
+            zfirst[z.zone_id] = first
+            first += len(z.c0)
+        for z in mesh.face_zones:  # face trees of adapted meshes
+            if z.bc_type != 31:
+                continue
+            cz, kids = mesh.face_children[z.zone_id]
+            f.write("(59 (%x %x %x %x)(\n" % (zfirst[z.zone_id], zfirst[z.zone_id] + len(z.c0) - 1, z.zone_id, cz))
+            np.savetxt(f, np.concatenate([np.full((len(kids), 1), 2), kids + zfirst[cz]], axis=1), fmt="%x")
+            f.write("))\n")
+        total = mesh.ncells + mesh.nparents
+        f.write("\n(12 (0 1 %x 0))\n" % total)
         f.write("(12 (%x 1 %x 1 %x))\n\n" % (CELL_ZONE, mesh.ncells, mesh.cell_type))
+        if mesh.nparents:
+            f.write("(12 (%x %x %x 20 %x))\n" % (PARENT_CELL_ZONE, mesh.ncells + 1, total, mesh.cell_type))
+            f.write("(58 (%x %x %x %x)(\n" % (mesh.ncells + 1, total, PARENT_CELL_ZONE, CELL_ZONE))
+            np.savetxt(f, np.concatenate([np.full((mesh.nparents, 1), 4), mesh.cell_children + 1], axis=1),
+                       fmt="%x")
+            f.write("))\n\n")
         f.write('(0 "Zones:")\n')
         f.write("(39 (%d fluid fluid)())\n" % CELL_ZONE)
         for z in mesh.face_zones:
+            if z.bc_type == 31:
+                continue  # parent face zones carry no name, as in Fluent's adapted meshes
             kind = "interior" if z.bc_type == 2 else "wall"
             f.write("(39 (%d %s %s)())\n" % (z.zone_id, kind, z.name))
 

@@ -22,7 +22,7 @@ import time
 
 import numpy as np
 
-from . import _lib
+from . import _lib, meshgen
 from ._lib import PsstError, Scheme, check
 
 __all__ = ["Grid", "Solver", "GridFV", "Scheme", "PsstError"]
@@ -59,7 +59,7 @@ class Grid:
         c0 = np.ascontiguousarray(np.concatenate([z.c0 for z in fz]).astype(np.int64))
         c1 = np.ascontiguousarray(np.concatenate([z.c1 for z in fz]).astype(np.int64))
         verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
-        zones = (_lib.ZoneDesc * (len(fz) + 1))()
+        zones = (_lib.ZoneDesc * (len(fz) + 2))()
         first = 1
         names = []
         for i, z in enumerate(fz):
@@ -69,8 +69,13 @@ class Grid:
             first += n
         names.append(b"fluid")
         zones[len(fz)] = _lib.ZoneDesc(2, 1, 1, mesh.ncells, names[-1])
+        nz = len(fz) + 1
+        if mesh.nparents:  # adapted mesh: the parent cells' zone (its trees stay with the file form)
+            zones[nz] = _lib.ZoneDesc(meshgen.PARENT_CELL_ZONE, 32, mesh.ncells + 1, mesh.ncells + mesh.nparents,
+                                      b"")
+            nz += 1
         d = _lib.FluentDesc(mesh.dim, len(verts), verts.ctypes.data, len(c0), face_ptr.ctypes.data,
-                            nodes.ctypes.data, c0.ctypes.data, c1.ctypes.data, mesh.ncells, len(fz) + 1,
+                            nodes.ctypes.data, c0.ctypes.data, c1.ctypes.data, mesh.ncells + mesh.nparents, nz,
                             ctypes.cast(zones, ctypes.POINTER(_lib.ZoneDesc)))
         h = ctypes.c_void_p()
         check(L.psst_grid_from_fluent(ctypes.byref(d), ctypes.byref(h)))
@@ -100,11 +105,12 @@ class Grid:
     def min_vol(self):
         return self._info.min_vol
 
-    _INT = {"face_c0", "face_c1", "face_zone", "vol_zone", "vol_boundary"}
+    _INT = {"face_c0", "face_c1", "face_zone", "vol_zone", "vol_boundary", "vol_bc"}
     _SIZES = {"vol_V": ("nvol", 1), "vol_x": ("nvol", "dim"), "face_S": ("nface", 1),
               "face_n": ("nface", "dim"), "face_x": ("nface", "dim"), "face_beta": ("nface", 1),
               "face_c0": ("nface", 1), "face_c1": ("nface", 1), "face_zone": ("nface", 1),
-              "vol_zone": ("nvol", 1), "vol_boundary": ("nvol", 1)}
+              "vol_zone": ("nvol", 1), "vol_boundary": ("nvol", 1),
+              "vol_bc": ("nvol", 1)}
 
     def get(self, name):
         n, w = self._SIZES[name]
@@ -288,6 +294,30 @@ class Solver:
             pass
 
 
+def write_sav(grid, prim, iteration, path):
+    """The .sav restart file of psstGridFV::private_save_solution
+    (psstFiniteVolumeGrid.cpp:606-639): the iteration, then per interior zone
+    (bc 1, ascending id; parent cells skipped) its id, its size and one line
+    p T u v (w) per cell, and a closing 0."""
+    nv, dim = grid.nvol, grid.dim
+    zone, vbc = grid.get("vol_zone"), grid.get("vol_bc")
+    with open(path, "w") as f:
+        f.write("%d\n" % iteration)
+        v = 0
+        while v < nv:
+            e = v
+            while e < nv and zone[e] == zone[v]:
+                e += 1
+            if vbc[v] == 1:
+                f.write("%d\n%d\n" % (zone[v], e - v))
+                for i in range(v, e):
+                    f.write("%.11f %.11f " % (prim[i], prim[nv + i]))
+                    f.write("".join("%.11f " % prim[(2 + k) * nv + i] for k in range(dim)))
+                    f.write("\n")
+            v = e
+        f.write("0")
+
+
 class GridFV:
     """The reference's driver flow (main.cpp + psstGridFV) on the GPU.
 
@@ -323,26 +353,10 @@ class GridFV:
 
     def save_solution(self, path, iteration):
         """Writes <case>.cas/<case>.dat (psstOutputManager.cpp) and the .sav
-        format of psstFiniteVolumeGrid.cpp:606-639 (psstGridFV::save_data)."""
+        (psstGridFV::save_data, psstFiniteVolumeGrid.cpp:240-245)."""
         prim = self.solver.get_state()
         self.grid.write_fluent(prim, self.solver.get("rho"), path[:-4] if path.endswith(".sav") else path)
-        nv, dim = self.grid.nvol, self.grid.dim
-        zone, bnd = self.grid.get("vol_zone"), self.grid.get("vol_boundary")
-        with open(path, "w") as f:
-            f.write("%d\n" % iteration)
-            v = 0
-            while v < nv:
-                e = v
-                while e < nv and zone[e] == zone[v]:
-                    e += 1
-                if not bnd[v]:
-                    f.write("%d\n%d\n" % (zone[v], e - v))
-                    for i in range(v, e):
-                        f.write("%.11f %.11f " % (prim[i], prim[nv + i]))
-                        f.write("".join("%.11f " % prim[(2 + k) * nv + i] for k in range(dim)))
-                        f.write("\n")
-                v = e
-            f.write("0")
+        write_sav(self.grid, prim, iteration, path)
 
     def explicit_solve(self, chunk=200):
         sc = self.scheme

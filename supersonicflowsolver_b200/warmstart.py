@@ -73,7 +73,7 @@ def solve_batch(cases, precision, flux, limiter, max_iter, chunk, init=None, sca
 def samples(case, grid, prim):
     """(inputs, targets) of one converged case's interior cells."""
     nv = grid.nvol
-    interior = grid.get("vol_boundary") == 0
+    interior = grid.get("vol_bc") == 1
     xy = grid.get("vol_x").reshape(nv, 2)[interior]
     p, T = prim[:nv][interior], prim[nv:2 * nv][interior]
     u, v = prim[2 * nv:3 * nv][interior], prim[3 * nv:][interior]
@@ -87,7 +87,7 @@ def predict_prim(net, case, grid, prim):
     import torch
 
     nv = grid.nvol
-    interior = grid.get("vol_boundary") == 0
+    interior = grid.get("vol_bc") == 1
     xy = grid.get("vol_x").reshape(nv, 2)[interior]
     x = torch.from_numpy(normalise_inputs(case["mach"], case["angle"], xy)).cuda()
     y = net.forward(x).cpu().numpy()

@@ -30,7 +30,7 @@ _ensure_built()
 
 
 def walls(mesh):
-    return [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
+    return [z.name for z in mesh.face_zones if z.bc_type not in (2, 31) and z.name not in ("in", "out", "side")]
 
 
 def make_case(tmpdir, mesh, name="t", **kw):

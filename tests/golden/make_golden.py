@@ -7,7 +7,7 @@ the reference printed. The mesh and case files are regenerated from the stored
 parameters, so the fixtures stay small and need no reference files at test time.
 
 Usage (needs oracle/_ref, i.e. the reference sources at build time):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names; default: all]
 """
 import json
 import os
@@ -38,6 +38,11 @@ GOLDEN = {
     "g2d_hll_first_order_rk1": ({"kind": "wedge2d", "nx": 40, "ny": 12, "angle_deg": 15.0},
                                 {"flux": 2, "order": 1, "limiter": 3, "grad": 1, "lc": 1, "rk_level": 1,
                                  "cfl": 2.08, "mach": 2.5}, 100),
+    # hanging-node mesh: parent cells and faces, quads with five faces
+    "g2d_adapted_hllc_lsq_vanleer": ({"kind": "wedge2d_adapted", "nx": 40, "ny": 12, "angle_deg": 15.0,
+                                      "refine_frac": 0.2, "seed": 3},
+                                     {"flux": 3, "order": 2, "limiter": 3, "grad": 2, "lc": 2, "rk_level": 4,
+                                      "cfl": 0.5, "mach": 2.5}, 20),
 }
 
 
@@ -51,17 +56,19 @@ def write_inputs(d, mesh_spec, case_kw, n_iter, name="g"):
     mesh = build_mesh(mesh_spec)
     path = os.path.join(d, "m.msh")
     meshgen.write_fluent(mesh, path)
-    zones = [z.name for z in mesh.face_zones if z.bc_type != 2 and z.name not in ("in", "out", "side")]
+    zones = [z.name for z in mesh.face_zones if z.bc_type not in (2, 31) and z.name not in ("in", "out", "side")]
     meshgen.write_case(d, name, dim=mesh.dim, zones=zones, max_iter=n_iter, **case_kw)
     return mesh, path
 
 
-def main():
+def main(names=()):
     for key, (mspec, ckw, n) in GOLDEN.items():
+        if names and key not in names:
+            continue
         with tempfile.TemporaryDirectory() as d:
             mesh, path = write_inputs(d, mspec, ckw, n)
             out = run_reference(path, d, "g", os.path.join(d, "dump"))
-            interior = out["vol_boundary"] == 0
+            interior = out["vol_bc"] == 1  # interior cells (not ghosts, not parent cells)
             dim = int(out["dim"][0])
             res = np.loadtxt(os.path.join(d, "g_residual.dat"))
             np.savez_compressed(
@@ -73,4 +80,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -47,12 +47,16 @@ CASES = [
     ("3d_tets_ausm_minmod_lc2", "t", dict(flux=1, order=2, limiter=2, lc=2, mach=3.0), 3),
     ("3d_hexes_hll_minmod_lc2", "h", dict(flux=2, order=2, limiter=2, lc=2, mach=3.0), 3),
     ("3d_hexes_ausm_first_uniform", "h", dict(flux=1, order=1, lc=0, mach=3.0), 4),
+    ("2d_adapted_hllc_vanleer", "a", dict(flux=3, order=2, limiter=3, lc=1), 4),
+    ("2d_adapted_ausm_lsq_vanalbada_lc2", "a", dict(flux=1, order=2, limiter=1, lc=2, grad=2), 4),
+    ("2d_adapted_hllc_bj", "a", dict(flux=3, order=2, limiter=4, lc=1), 4),
 ]
 MESH = {
     "q": lambda: meshgen.wedge2d(30, 10, 15.0),
     "j": lambda: meshgen.wedge2d(30, 10, 15.0, jitter=0.15, seed=3, shuffle_seed=1, interior_first=True),
     "t": lambda: meshgen.wedge3d(10, 5, 3, 12.0, tets=True),
     "h": lambda: meshgen.wedge3d(10, 5, 3, 12.0, tets=False, interior_first=True),
+    "a": lambda: meshgen.wedge2d_adapted(30, 10, 15.0, refine_frac=0.2, seed=5),  # hanging nodes
 }
 
 
@@ -63,7 +67,7 @@ def test_fp64_bit_exact_per_iteration(tmp_path, tag, mesh, ckw, n, renumber):
     path, d, name = make_case(tmp_path, m, max_iter=n, **ckw)
     g, s = gpu_solver(path, d, name, renumber=renumber)
     o = Oracle(path, d, name)
-    interior = o.get("vol_boundary") == 0
+    interior = o.get("vol_bc") == 1
     nvol, dim = g.nvol, g.dim
     for it in range(n):
         linf, _ = s.explicit_solve(1)
@@ -98,7 +102,7 @@ def test_fp64_matches_reference_golden(tmp_path, fixture):
     linf, _ = s.explicit_solve(prm["iterations"])
     prim = s.get_state()
     nv, dim = g.nvol, g.dim
-    interior = g.get("vol_boundary") == 0
+    interior = g.get("vol_bc") == 1
     assert np.array_equal(prim[:nv][interior], z["p"])
     assert np.array_equal(prim[nv:2 * nv][interior], z["T"])
     assert np.array_equal(prim[2 * nv:].reshape(dim, nv).T[interior], z["u"])
@@ -121,7 +125,7 @@ def test_fp64_cell_limiters_match_oracle(tmp_path, limiter, mesh):
     assert np.array_equal(linf, olinf)
     assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim))
     np.testing.assert_allclose(l2, ol2, rtol=1e-12, atol=0)
-    interior = o.get("vol_boundary") == 0
+    interior = o.get("vol_bc") == 1
     lim = s.get("limiter").reshape(g.nvol, -1)[interior]
     assert np.array_equal(lim, o.get("vol_lim").reshape(g.nvol, -1)[interior])
 
@@ -223,7 +227,7 @@ def test_fp32_close_to_fp64_oracle(tmp_path, flux):
     o.run(30)
     a, b = s.get_state(), oracle_prim(o, g.nvol, g.dim)
     nv = g.nvol
-    interior = o.get("vol_boundary") == 0
+    interior = o.get("vol_bc") == 1
     for sl, tol in ((slice(0, nv), 2e-4), (slice(nv, 2 * nv), 2e-4)):
         x, y = a[sl][interior], b[sl][interior]
         assert np.max(np.abs(x - y) / np.abs(y)) < tol

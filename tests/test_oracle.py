@@ -43,7 +43,7 @@ def test_oracle_matches_reference_golden(tmp_path, fixture):
     z, prm, mesh, path = build_golden_inputs(tmp_path, fixture)
     o = Oracle(path, str(tmp_path), "g")
     linf, _ = o.run(prm["iterations"])
-    interior = o.get("vol_boundary") == 0
+    interior = o.get("vol_bc") == 1
     assert np.array_equal(o.get("vol_p")[interior], z["p"])
     assert np.array_equal(o.get("vol_T")[interior], z["T"])
     assert np.array_equal(o.get("vol_u").reshape(-1, mesh.dim)[interior], z["u"])
