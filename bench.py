@@ -150,15 +150,17 @@ def traffic_model(grid, nnz, kind):
     K = nnz / nint
     if kind == "face":
         # per face: face record read (64: c0,c1 (2i), S (g), n (3g), two FP32 offset vectors)
-        # and the face output record written (48: flux*area 5s, time-step terms 7s);
+        # and the face output record written (32: flux*area 5s, time-step terms 3s);
         # per interior cell: state record (32) + gradient/limiter record (80); ghosts: state (32)
-        return nf * (64 + 48) + nint * (32 + 80) + ngh * 32
+        return nf * (64 + 32) + nint * (32 + 80) + ngh * 32
     if kind == "cell":
         # per cell: CSR ptr (i) + K entries (i) + K face areas (s) + own-order perm (8) + V (g) +
-        # w, prev_w (FP64 2x5x8, a third more on stage 0 amortised) + new state record (32) + dt
-        # (g) + ghost ptr (i); per face: face output record (48); per ghost: record in and out
-        # (2x32) + ids (2i)
-        return nint * (4 + 4 * K + 4 * K + 8 + 8 + 90 + 32 + 8 + 4) + nf * 48 + ngh * 72
+        # the stage-start FP64 state read (5x8) + new state record (32) + ghost ptr (i), and,
+        # averaged over the S stages of an iteration, the stage-start copy written on the first
+        # stage and w and dt written on the last (5x8 + 5x8 + 8) / S; per face: face output
+        # record (32); per ghost: record in and out (2x32) + ids (2i)
+        S = SCHEME["rk_level"]
+        return nint * (4 + 4 * K + 4 * K + 8 + 8 + 40 + 88.0 / S + 32 + 4) + nf * 32 + ngh * 72
     if kind == "gradient":
         # per cell: CSR (i + K i) + perm + V + eps^2 + own state record (32) + gradient/limiter
         # record written (80); per face: face record (64) + beta (g); ghosts: state record (32)
@@ -340,6 +342,11 @@ def run_gpu(args):
 
     # warm-up
     solver.explicit_solve(args.warmup)
+    if solver.graphs_on:  # capture the timed call's graphs (one per buffer parity) outside the timed region
+        solver.explicit_solve(args.steps)
+        solver.explicit_solve(args.steps)
+        solver.explicit_solve(1)
+        solver.explicit_solve(1)
     barrier()
     # device-resident timed region; inputs (~2.6 GB of mesh + state) exceed the 126 MB L2
     with ClockSampler(dev) as clk:

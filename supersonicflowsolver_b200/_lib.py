@@ -8,7 +8,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libpsst_b200.so")
+# PSST_B200_LIB selects another build of the library (e.g. one compiled with
+# other register budgets); default: the in-tree build.
+LIB_PATH = os.environ.get("PSST_B200_LIB") or os.path.join(HERE, "_build", "libpsst_b200.so")
 
 PSST_OK = 0
 STATUS_NAMES = {1: "PSST_ERR_ARG", 2: "PSST_ERR_IO", 3: "PSST_ERR_FORMAT", 4: "PSST_ERR_CUDA",

@@ -38,15 +38,24 @@ struct alignas(16) FaceRec {
 };
 
 // Output of the face pass for one face: flux * area (DIM+2), then the face's
-// local-time-step terms: for LocalAccTime1 the products u0.n and u1.n of the
-// two neighbours' velocities with the normal (DIM each) and the mean sound
-// speed (the face area comes from DevGrid::csr_s); for LocalAccTime2 S |n_k|
-// (DIM). 12 values: 48 bytes in FP32, 96 in FP64.
+// local-time-step terms: for LocalAccTime1 the two neighbours' normal
+// velocities and the mean sound speed (the face area comes from
+// DevGrid::csr_s); for LocalAccTime2 S |n_k| (DIM values from Q0). The normal
+// velocities are kept per component (u_k n_k, NQ = DIM per side) on the FP64
+// path, because the reference adds the neighbour's components one at a time
+// onto a value carried over from the previous face
+// (psstLocalTimeCalculation.cpp:117-124), and as their sums (NQ = 1) on the
+// FP32 path: 12 values (96 bytes) in FP64, 8 (32 bytes) in FP32.
+#ifndef PSST_FACEOUT_COMPACT
+#define PSST_FACEOUT_COMPACT 1
+#endif
 template <typename R, int DIM>
 struct alignas(16) FaceOut {
+    static constexpr bool COMPACT = sizeof(R) == 4 && PSST_FACEOUT_COMPACT;
     static constexpr int NV = DIM + 2;
-    static constexpr int Q0 = NV, Q1 = NV + DIM, CN = NV + 2 * DIM;
-    R v[12];
+    static constexpr int NQ = COMPACT ? 1 : DIM;
+    static constexpr int Q0 = NV, Q1 = NV + NQ, CN = NV + 2 * NQ;
+    R v[COMPACT ? 8 : 12];
 };
 
 struct DevGrid {

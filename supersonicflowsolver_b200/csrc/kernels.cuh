@@ -22,6 +22,19 @@
 
 #include "devgrid.hpp"
 
+// Register budgets of the three hot kernels (compile-time tuning; the values
+// are the measured best on the 6M-tet benchmark): k_face register cap,
+// k_cell and k_gradient minimum resident 256-thread blocks per SM.
+#ifndef PSST_FACE_MAXNREG
+#define PSST_FACE_MAXNREG 72
+#endif
+#ifndef PSST_CELL_MINB
+#define PSST_CELL_MINB 4
+#endif
+#ifndef PSST_GRAD_MINB
+#define PSST_GRAD_MINB 1
+#endif
+
 namespace psst {
 
 enum ErrCode { ERR_HLL = 1, ERR_HLLC = 2, ERR_NONFINITE_RES = 3, ERR_BAD_STATE = 4 };
@@ -323,9 +336,9 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
 //   reference adds the two sound speeds in the opposite order on the other
 //   side; IEEE addition is commutative) and S;
 //  LocalAccTime2 (:189-193): S |n_k|.
-// At most 72 registers: seven 128-thread blocks per SM (the tuned shape).
+// Register cap PSST_FACE_MAXNREG (72: seven 128-thread blocks per SM, the tuned shape).
 template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
-__global__ void __maxnreg__(72) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
+__global__ void __maxnreg__(PSST_FACE_MAXNREG) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     using FO = FaceOut<R, DIM>;
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
@@ -361,10 +374,21 @@ __global__ void __maxnreg__(72) k_face(DevGrid g, DevState<R> st, DevWork<R> wk,
     for (int j = 0; j < DIM + 2; ++j) o.v[j] = flow[j] * S;
     if (LC == 1) {
         const R gr = (R)gas.gamma * (R)gas.rm;
+        if (FO::NQ == DIM) {
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            o.v[FO::Q0 + k] = p0.u[k] * nn[k];
-            o.v[FO::Q1 + k] = p1.u[k] * nn[k];
+            for (int k = 0; k < DIM; ++k) {
+                o.v[FO::Q0 + k] = p0.u[k] * nn[k];
+                o.v[FO::Q1 + k] = p1.u[k] * nn[k];
+            }
+        } else {
+            R a = (R)0, b = (R)0;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                a += p0.u[k] * nn[k];
+                b += p1.u[k] * nn[k];
+            }
+            o.v[FO::Q0] = a;
+            o.v[FO::Q1] = b;
         }
         o.v[FO::CN] = (sqrt(gr * p1.T) + sqrt(gr * p0.T)) * (R)0.5;
     } else if (LC == 2) {
@@ -386,7 +410,7 @@ __global__ void __maxnreg__(72) k_face(DevGrid g, DevState<R> st, DevWork<R> wk,
 // Venkatakrishnan (AIAA 93-0880) cell limiter:
 // psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c).
 template <typename R, int DIM, int GRAD, int CELLLIM>
-__global__ void __launch_bounds__(256) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
+__global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
     constexpr int NVAR = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nint) return;
@@ -580,10 +604,13 @@ __device__ __forceinline__ RkIn<NV> rk_load(const DevGrid &g, const DevWork<R> &
 
 // RK stage update of one cell given its residual (psstFiniteVolumeGrid.cpp:324-346):
 // w = prev_w - dt*a*res/V in FP64, primitives, norms; returns the new record.
+// w and dt are stored only when `keep` is set: inside a whole iteration only
+// the last stage's values are ever read (the next iteration's first stage
+// loads w; stages 2.. load the stage-start copy pw).
 template <typename R, int DIM>
 __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<R> &wk, const Gas &gas,
                                                 const RkIn<DIM + 2> &in, double dt, double alpha, int first_stage,
-                                                int32_t c, const R res[DIM + 2], double sq[DIM + 2],
+                                                bool keep, int32_t c, const R res[DIM + 2], double sq[DIM + 2],
                                                 double mx[DIM + 2]) {
     constexpr int NV = DIM + 2;
     const double vol = in.vol;
@@ -594,7 +621,7 @@ __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<
         const double pw = in.pw[v];
         if (first_stage) wk.pw[idx] = pw;
         w[v] = pw - dt * alpha * (double)res[v] / vol;
-        wk.w[idx] = w[v];
+        if (keep) wk.w[idx] = w[v];
         const double rv = (double)res[v];
         const double ar = fabs(rv);
         if (mx[v] < ar) mx[v] = ar;  // NaN never replaces the max, as in `if (res < |r|)` (:331)
@@ -613,7 +640,7 @@ __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<
     const double T = ((w[DIM + 1] / rho) - (vs * 0.5)) / gas.cv;
     const double p = rho * gas.rm * T;
     if (!(rho > 0.0 && T > 0.0)) flag_error(wk.err, ERR_BAD_STATE, c);
-    wk.dt[c] = dt;
+    if (keep) wk.dt[c] = dt;
     return pack<R, DIM>((R)p, (R)T, (R)rho, u);
 }
 
@@ -801,11 +828,33 @@ __device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<
 // At least 4 blocks of 256 per SM (64 registers): the pass is bound by the
 // latency of its gathers, and the occupancy gained outweighs a 24-byte spill
 // (0.61 -> 0.56 ms per launch on 6M tets, FP32).
-template <typename R, int DIM, int LC, bool BATCH>
-__global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
-                                              double cfl, double dt_uniform, double alpha, int first_stage,
-                                              int it_slot) {
+// LocalAccTime1 face terms seen from one side: returns the cell's own u . n
+// and adds the neighbour's u . n onto the running value nnb, component by
+// component where the record keeps components (the reference's order,
+// psstLocalTimeCalculation.cpp:117-124).
+template <typename R, int DIM>
+__device__ __forceinline__ R lc1_normal_velocities(const FaceOut<R, DIM> &o, int side, R &nnb) {
     using FO = FaceOut<R, DIM>;
+    if (FO::NQ == DIM) {
+        R nv = (R)0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            nv += side ? o.v[FO::Q1 + k] : o.v[FO::Q0 + k];
+            nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];
+        }
+        return nv;
+    }
+    nnb += side ? o.v[FO::Q0] : o.v[FO::Q1];
+    return side ? o.v[FO::Q1] : o.v[FO::Q0];
+}
+
+template <typename R, int DIM, int LC, bool BATCH>
+__global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
+                                              double cfl, double dt_uniform, double alpha, int stage,
+                                              int it_slot) {
+    // stage: bit 0 first stage of the iteration, bit 1 last stage
+    using FO = FaceOut<R, DIM>;
+    const int first_stage = stage & 1;
     constexpr int NV = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     double sq[NV], mx[NV];
@@ -847,12 +896,7 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
             }
             if (one_pass) {
                 if (LC == 1) {
-                    R nv = (R)0;
-#pragma unroll
-                    for (int k = 0; k < DIM; ++k) {
-                        nv += side ? o.v[FO::Q1 + k] : o.v[FO::Q0 + k];
-                        nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];
-                    }
+                    const R nv = lc1_normal_velocities<R, DIM>(o, side, nnb);
                     nnb = (nnb + nv) * (R)0.5;
                     den += (fabs(nnb) + o.v[FO::CN]) * csr_s[b + q];
                 } else if (LC == 2) {
@@ -869,12 +913,7 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
                     const int32_t ent = g.csr_ent[slot];
                     const FO o = ld16(fo + (ent >> 1));
                     const int side = ent & 1;
-                    R nv = (R)0;
-#pragma unroll
-                    for (int k = 0; k < DIM; ++k) {
-                        nv += side ? o.v[FO::Q1 + k] : o.v[FO::Q0 + k];   // own u . n
-                        nnb += side ? o.v[FO::Q0 + k] : o.v[FO::Q1 + k];  // neighbour u . n
-                    }
+                    const R nv = lc1_normal_velocities<R, DIM>(o, side, nnb);
                     nnb = (nnb + nv) * (R)0.5;
                     den += (fabs(nnb) + o.v[FO::CN]) * csr_s[slot];
                 }
@@ -893,7 +932,8 @@ __global__ void __launch_bounds__(256, 4) k_cell(DevGrid g, DevState<R> cur, Dev
             }
             dt = (double)((R)cfl * (R)g.V[c] / den);
         }
-        const CellRec<R> nrec = rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, c, res, sq, mx);
+        const CellRec<R> nrec = rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, (stage & 2) != 0, c, res,
+                                                  sq, mx);
         st16(nxt.rec + c, nrec);
         const int32_t g0 = g.gptr[c], g1 = g.gptr[c + 1];
         if (g1 > g0) {
@@ -932,7 +972,7 @@ __device__ __forceinline__ void update_from_buffers(const DevGrid &g, const DevS
         dt = local_time<R, DIM, 1, true>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
     else
         dt = local_time<R, DIM, LC, false>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);
-    st16(nxt.rec + c, rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, c, res, sq, mx));
+    st16(nxt.rec + c, rk_update<R, DIM>(g, wk, gas, rin, dt, alpha, first_stage, true, c, res, sq, mx));
 }
 
 template <typename R, int DIM, int LC, bool GATHER>

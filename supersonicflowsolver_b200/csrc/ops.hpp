@@ -41,7 +41,7 @@ struct Ops {
     // residual, time step, RK update, ghosts, norms (last block finishes them)
     static void cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                      const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
-                     int first_stage, int it_slot, cudaStream_t s);
+                     int stage, int it_slot, cudaStream_t s);  // stage: 1 first, 2 last (bits)
     static void residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStream_t s);
     // cell update from face outputs (gather) or from wk.res; seq: the
     // sequential LocalAccTime1 (single block over levels); norms by norm_finish

@@ -160,13 +160,13 @@ static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevSt
 
 template <typename R>
 void Ops<R>::cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
-                  const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha, int first_stage,
+                  const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha, int stage,
                   int it_slot, cudaStream_t s) {
     if (g.nint == 0) return;
     if (dim == 2)
-        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, it_slot, s);
     else
-        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, first_stage, it_slot, s);
+        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, it_slot, s);
 }
 
 template <typename R>

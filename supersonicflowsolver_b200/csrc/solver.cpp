@@ -536,7 +536,8 @@ void one_stage(psst_solver *s, int k, int it_slot, bool gather, Mark &&mark) {
         mark(K_FACE);
     }
     if (gather && !s->seq) {
-        Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], k == 0,
+        const int stage = (k == 0 ? 1 : 0) | (k == s->sc.rk_level - 1 ? 2 : 0);
+        Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], stage,
                      it_slot, s->stream);
         mark(K_CELL);
     } else {

@@ -255,6 +255,9 @@ class Solver:
     def use_graphs(self, on=True):
         """Capture each explicit_solve call as a CUDA graph and replay it."""
         check(_lib.load().psst_solver_use_graphs(self._h, int(bool(on))))
+        self.graphs_on = bool(on)
+
+    graphs_on = False
 
     def set_active(self, flags):
         """Merged grids: per-case run flags (stopped cases keep their state)."""

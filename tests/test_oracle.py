@@ -79,8 +79,35 @@ def test_oracle_matches_compiled_reference_3d(tmp_path, tets):
     _check_vs_reference(tmp_path, mesh, dict(flux=3, order=2, limiter=3, lc=1, mach=3.0), 3)
 
 
+@pytest.mark.skipif(not reference_available(), reason="compiled reference not built here")
+@pytest.mark.parametrize("grad", [1, 2], ids=["green_gauss", "least_squares"])
+def test_oracle_matches_compiled_reference_adapted(tmp_path, grad):
+    """Hanging-node mesh (parent cells and faces, five-face quads)."""
+    mesh = meshgen.wedge2d_adapted(24, 8, 15.0, refine_frac=0.25, seed=7)
+    _check_vs_reference(tmp_path, mesh, dict(flux=3, order=2, limiter=3, lc=1, grad=grad), 4)
+
+
+@pytest.mark.skipif(not (reference_available() and os.path.exists(os.path.join(REFERENCE_DIR, "testGrids"))),
+                    reason="reference not mounted")
+@pytest.mark.parametrize("mesh", ["quad2D_adapted1.msh", "quad2D_adapted2.msh"])
+def test_oracle_matches_reference_on_its_adapted_samples(tmp_path, mesh):
+    """The reference's own hanging-node samples (testGrids/guads): far-field
+    inlet/outlet as 23/26, walls 15/18."""
+    src = os.path.join(REFERENCE_DIR, "testGrids", "guads", mesh)
+    (tmp_path / "m.msh").write_bytes(open(src, "rb").read().replace(b"\r", b""))
+    meshgen.write_case(str(tmp_path), "c", max_iter=4, flux=3, order=2, limiter=3, lc=1, zones=())
+    vel = open(tmp_path / "c.par").read().split("\t")[0]
+    (tmp_path / "c.bvp").write_text("inlet\t23\t%s\t101325\noutlet\t26\nup\t15\ndown\t15" % vel.replace(" ", "\t"))
+    (tmp_path / "c.btq").write_text("inlet\t27\t300\noutlet\t25\nup\t18\ndown\t18")
+    _check_vs_reference_files(str(tmp_path / "m.msh"), str(tmp_path), "c", 4)
+
+
 def _check_vs_reference(tmp_path, mesh, ckw, n):
     path, d, name = make_case(tmp_path, mesh, max_iter=n, **ckw)
+    _check_vs_reference_files(path, d, name, n)
+
+
+def _check_vs_reference_files(path, d, name, n):
     ref = run_reference(path, d, name, os.path.join(d, "dump"))
     o = Oracle(path, d, name)
     o.run(n)
