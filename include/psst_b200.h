@@ -362,6 +362,10 @@ psst_status psst_mlp_gradients(psst_mlp *m, const float *x, const float *t, int 
 /* One Adam step (beta 0.9/0.999, eps 1e-8) at learning rate lr; returns the loss
  * before the step. */
 psst_status psst_mlp_train_step(psst_mlp *m, const float *x, const float *t, int B, float lr, float *loss);
+/* The network's kernels run on `stream` (a cudaStream_t; NULL: its own
+ * non-blocking stream). x, t and y are device arrays read and written in
+ * stream order: inputs produced on another stream must be complete before a
+ * call, and y of psst_mlp_forward is complete only in `stream`'s order. */
 psst_status psst_mlp_set_stream(psst_mlp *m, void *stream);
 void psst_mlp_destroy(psst_mlp *m);
 

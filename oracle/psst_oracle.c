@@ -70,7 +70,7 @@ struct oracle {
     int lc, rk_level, flux, order, gradm, limiter, lc1_jacobi;
     double rk[64];
     double venkat_k;
-    double *lsq_r; /* 3 coefficients per zone-local index (quirk of psstLeastSquare) */
+    double *lsq_r; /* LSQ_NR coefficients per zone-local index (quirk of psstLeastSquare) */
     long lsq_n;
     double *lim; /* per volume x NG limiter value (BJ/VK extension) */
 };
@@ -883,37 +883,51 @@ static void gg_initialize(oracle_t *o) {
     free(bz);
 }
 
-/* psstLeastSquare::initialize (:191-260), 2D; r_ indexed by zone position. */
+/* psstLeastSquare::initialize (:191-260); r_ indexed by zone position.
+ * Coefficients per index: r11, r12, r22 and, in 3D, r13, r23, r33 and beta
+ * (the Gram-Schmidt factors of the weighted normal equations, w = 1/|dx|^2;
+ * Anderson & Bonhaus, Computers & Fluids 23 (1994) 1-21), computed as the
+ * reference computes them for both dimensions. */
+#define LSQ_NR 7
 static int lsq_initialize(oracle_t *o) {
-    if (o->dim != 2)
-        return fail(o, "least-squares gradient: the reference's 3D path writes out of bounds "
-                       "(psstGradCalculation.cpp:338); only 2D is supported");
+    int dim = o->dim;
     long maxc = 0;
     for (long i = 0; i < o->nvz; ++i)
         if (o->vz[i].bc == 1 && o->vz[i].count > maxc) maxc = o->vz[i].count;
     o->lsq_n = maxc;
-    o->lsq_r = (double *)calloc(3 * (maxc + 1), sizeof(double));
+    o->lsq_r = (double *)calloc(LSQ_NR * (maxc + 1), sizeof(double));
     for (long zi = 0; zi < o->nvz; ++zi) {
         if (o->vz[zi].bc != 1) continue;
         for (long i = 0; i < o->vz[zi].count; ++i) {
             long v = o->vz[zi].first_vol + i;
-            double ca = 0.0, cb = 0.0, cd = 0.0;
+            double ca = 0.0, cb = 0.0, cd = 0.0, cc = 0.0, ce = 0.0, cg = 0.0;
             for (long j = 0; j < o->v_fcnt[v]; ++j) {
                 long nb = face_other(o, o->v_f[v][j], v);
-                double diff[2], w = 0.0;
-                for (int k = 0; k < 2; ++k) {
-                    diff[k] = o->xc[nb * 2 + k] - o->xc[v * 2 + k];
+                double diff[3] = {0.0, 0.0, 0.0}, w = 0.0;
+                for (int k = 0; k < dim; ++k) {
+                    diff[k] = o->xc[nb * dim + k] - o->xc[v * dim + k];
                     w += diff[k] * diff[k];
                 }
                 double ws = 1.0 / w;
                 ca += ws * diff[0] * diff[0];
                 cb += ws * diff[0] * diff[1];
                 cd += ws * diff[1] * diff[1];
+                if (dim == 3) {
+                    cc += ws * diff[0] * diff[2];
+                    ce += ws * diff[1] * diff[2];
+                    cg += ws * diff[2] * diff[2];
+                }
             }
-            double *r = &o->lsq_r[3 * i];
+            double *r = &o->lsq_r[LSQ_NR * i];
             r[0] = sqrt(ca);
             r[1] = cb / r[0];
             r[2] = sqrt(cd - r[1] * r[1]);
+            if (dim == 3) {
+                r[3] = cc / r[0];
+                r[4] = (ce - r[1] / r[0] * cc) / r[2];
+                r[5] = sqrt(cg - (r[3] * r[3] + r[4] * r[4]));
+                r[6] = (r[1] * r[4] - r[3] * r[2]) / (r[0] * r[2]);
+            }
         }
     }
     return 0;
@@ -1065,21 +1079,26 @@ static void gg_calculate(oracle_t *o) {
     }
 }
 
-/* psstLeastSquare::calculate (:268-368), 2D */
+/* psstLeastSquare::calculate (:268-368). 2D as the reference. 3D is a
+ * corrected restatement: the reference leaves alpha[0..1] at zero and writes
+ * alpha[3] out of bounds (:338); here alpha_1, alpha_2 are the 2D ones and
+ * alpha_3 = (dz - r23/r22 dy + beta dx) / r33^2 (Anderson & Bonhaus 1994; the
+ * reference's beta * dz term would not reproduce linear fields), then the
+ * reference's theta corrections (:342-347). */
 static void lsq_calculate(oracle_t *o) {
-    int nvar = 5;
+    int dim = o->dim, nvar = dim + 3;
     for (long zi = 0; zi < o->nvz; ++zi) {
         if (o->vz[zi].bc != 1) continue;
         for (long i = 0; i < o->vz[zi].count; ++i) {
             long v = o->vz[zi].first_vol + i;
             for (int n = 0; n < nvar; ++n)
-                for (int k = 0; k < 2; ++k) grad_of(o, v, n)[k] = 0.0;
-            const double *r = &o->lsq_r[3 * i];
+                for (int k = 0; k < dim; ++k) grad_of(o, v, n)[k] = 0.0;
+            const double *r = &o->lsq_r[LSQ_NR * i];
             for (long j = 0; j < o->v_fcnt[v]; ++j) {
                 long nb = face_other(o, o->v_f[v][j], v);
-                double diff[2], w = 0.0, phi[5], alpha[2], theta[2];
-                for (int k = 0; k < 2; ++k) {
-                    diff[k] = o->xc[nb * 2 + k] - o->xc[v * 2 + k];
+                double diff[3], w = 0.0, phi[6], alpha[3], theta[3];
+                for (int k = 0; k < dim; ++k) {
+                    diff[k] = o->xc[nb * dim + k] - o->xc[v * dim + k];
                     w += diff[k] * diff[k];
                 }
                 for (int n = 0; n < nvar; ++n) phi[n] = (var_of(o, nb, n) - var_of(o, v, n));
@@ -1088,8 +1107,14 @@ static void lsq_calculate(oracle_t *o) {
                 alpha[1] = (diff[1] - r[1] / r[0] * diff[0]) / (r[2] * r[2]);
                 theta[0] = alpha[0] - r[1] / r[0] * alpha[1];
                 theta[1] = alpha[1];
+                if (dim == 3) {
+                    alpha[2] = (diff[2] - r[4] / r[2] * diff[1] + r[6] * diff[0]) / (r[5] * r[5]);
+                    theta[0] += alpha[2] * r[6];
+                    theta[1] -= r[4] / r[2] * alpha[2];
+                    theta[2] = alpha[2];
+                }
                 for (int n = 0; n < nvar; ++n)
-                    for (int k = 0; k < 2; ++k) grad_of(o, v, n)[k] += ws * theta[k] * phi[n];
+                    for (int k = 0; k < dim; ++k) grad_of(o, v, n)[k] += ws * theta[k] * phi[n];
             }
         }
     }

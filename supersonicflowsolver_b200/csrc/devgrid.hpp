@@ -73,7 +73,7 @@ struct DevGrid {
     const int32_t *csr_nb;    // the cell across each csr_ent face (saves a dependent load)
     const void *csr_s;        // R per csr_ent: the face's area, rounded to R (LocalAccTime1)
     const uint64_t *wperm;    // [nint] 4-bit slots: k-th face of the cell's own face order
-    const double *lsq_r;      // [3][nint] 2D least-squares coefficients (reference table)
+    const double *lsq_r;      // [3 (2D) or 7 (3D)][nint] least-squares coefficients (reference table)
     const double *vk_eps2;    // [nint] Venkatakrishnan epsilon^2 = (K h)^3, h = V^(1/dim)
     const int32_t *rank;      // [nint] position in the reference's interior update order
     const int32_t *gptr;      // [nint+1] ghosts of each interior cell (ghost index space)

@@ -163,7 +163,8 @@ void green_gauss_beta(psst_grid &g) {
     std::vector<double> bz((size_t)maxc + 1, 0.0);
     for (auto &z : g.fz) {
         if (z.bc == 31) continue;
-        for (int64_t i = 0; i < z.count; ++i) {
+        parallel_for(z.count, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
             const int64_t f = z.first + i;
             double d[2];
             for (int j = 0; j < 2; ++j) {
@@ -181,6 +182,7 @@ void green_gauss_beta(psst_grid &g) {
             }
             bz[i] = d[1] / (d[0] + d[1]);
         }
+        });
     }
     for (auto &z : g.fz)
         for (int64_t i = 0; i < z.count; ++i) g.beta[z.first + i] = bz[i];
@@ -262,13 +264,23 @@ psst_grid *build_grid(const RawMesh &m) {
 
     // Wiring in file zone order (psstAnsysGridReader.cpp:825-883): the order in
     // which faces are appended to a volume is its face order everywhere after.
+    // volume of every file cell (-1: its zone is no volume zone)
+    std::vector<int64_t> cell_vol(m.cell_zone.size(), -1);
+    for (auto &kv : vzs) {
+        const Zone &z = m.zones[kv.second];
+        const int64_t base = g.vz[vslot[z.id]].first;
+        for (int64_t c = 0; c < z.size; ++c)
+            if (z.first - 1 + c >= 0 && z.first - 1 + c < (int64_t)cell_vol.size() && m.cell_zone[z.first - 1 + c] == z.id)
+                cell_vol[z.first - 1 + c] = base + c;
+    }
     std::vector<int64_t> cnt(g.nvol, 0);
-    std::vector<std::pair<int64_t, int64_t>> adds;  // (volume, face), in wiring order
-    adds.reserve(2 * g.nface);
+    std::vector<int64_t> worder;  // faces in wiring order
+    worder.reserve(g.nface);
     for (size_t zi = 0; zi < m.zones.size(); ++zi) {
         const Zone &z = m.zones[zi];
         if (z.bc == 1 || z.bc == 32) continue;
         const int32_t fs = fslot[z.id];
+        const int64_t ghost0 = z.bc == 2 || z.bc == 31 ? -1 : g.vz[vslot[z.id]].first;
         for (int64_t j = 0; j < g.fz[fs].count; ++j) {
             const int64_t f = g.fz[fs].first + j;
             const int64_t loc = f_loc[f];
@@ -277,36 +289,41 @@ psst_grid *build_grid(const RawMesh &m) {
                 int64_t vol;
                 if (cell == 0) {
                     if (z.bc == 31) continue;
-                    vol = g.vz[vslot[z.id]].first + j;
+                    if (ghost0 < 0) raise(PSST_ERR_FORMAT, "mesh: interior face without two neighbours");
+                    vol = ghost0 + j;
                 } else {
                     if (cell - 1 >= (int64_t)m.cell_zone.size()) raise(PSST_ERR_FORMAT, "mesh: cell index out of range");
-                    const int64_t czone = m.cell_zone[cell - 1];
-                    auto it = vslot.find(czone);
-                    if (it == vslot.end()) raise(PSST_ERR_FORMAT, "mesh: face refers to a cell outside any cell zone");
-                    const Zone &cz = m.zones[vzs[czone]];
-                    vol = g.vz[it->second].first + (cell - cz.first);
+                    vol = cell_vol[cell - 1];
+                    if (vol < 0) raise(PSST_ERR_FORMAT, "mesh: face refers to a cell outside any cell zone");
                 }
                 (k == 0 ? g.f_c0[f] : g.f_c1[f]) = vol;
-                if (z.bc != 31) {
-                    adds.emplace_back(vol, f);
-                    ++cnt[vol];
-                }
+                if (z.bc != 31) ++cnt[vol];
             }
-            face_geometry(g, m, f, loc);
+            worder.push_back(f);
         }
     }
+    // face lists in wiring order: faces of zone 31 are in none
     g.vf_ptr.assign(g.nvol + 1, 0);
     for (int64_t v = 0; v < g.nvol; ++v) {
         g.vf_ptr[v + 1] = g.vf_ptr[v] + cnt[v];
         g.max_faces = std::max<int>(g.max_faces, (int)cnt[v]);
     }
     g.vf_idx.assign(g.vf_ptr[g.nvol], 0);
-    std::vector<int64_t> fill(g.vf_ptr.begin(), g.vf_ptr.end() - 1);
-    for (auto &a : adds) g.vf_idx[fill[a.first]++] = a.second;
+    {
+        std::vector<int64_t> fill(g.vf_ptr.begin(), g.vf_ptr.end() - 1);
+        for (int64_t f : worder) {
+            if (g.fz[g.f_fz[f]].bc == 31) continue;
+            if (g.f_c0[f] >= 0) g.vf_idx[fill[g.f_c0[f]]++] = f;
+            if (g.f_c1[f] >= 0) g.vf_idx[fill[g.f_c1[f]]++] = f;
+        }
+    }
+    parallel_for((int64_t)worder.size(), [&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) face_geometry(g, m, worder[i], f_loc[worder[i]]);
+    });
 
     g.V.assign(g.nvol, 0.0);
     g.xc.assign(g.nvol * dim, 0.0);
-    double mn = -1.0;  // psstAnsysGridReader.cpp:886-905
+    std::vector<int64_t> vorder;  // volumes in the reference's initialisation order
     for (size_t zi = 0; zi < m.zones.size(); ++zi) {
         const Zone &z = m.zones[zi];
         if (z.bc == 2 || z.bc == 31 || z.bc == 32) continue;
@@ -317,49 +334,68 @@ psst_grid *build_grid(const RawMesh &m) {
                 raise(PSST_ERR_FORMAT, "mesh: boundary zone " + std::to_string(z.id) +
                                            " has a face without a free side (no ghost cell)");
             if (!g.vol_boundary[v] && cnt[v] == 0) raise(PSST_ERR_FORMAT, "mesh: cell without faces");
-            volume_geometry(g, m, f_loc, v);
-            if (z.bc == 1 && (mn > g.V[v] || mn < 0.0)) mn = g.V[v];
+            vorder.push_back(v);
         }
     }
+    parallel_for((int64_t)vorder.size(), [&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) volume_geometry(g, m, f_loc, vorder[i]);
+    });
+    double mn = -1.0;  // psstAnsysGridReader.cpp:886-905
+    for (int64_t v : vorder)
+        if (g.vz[g.vol_vz[v]].bc == 1 && (mn > g.V[v] || mn < 0.0)) mn = g.V[v];
     g.min_vol = mn;
     green_gauss_beta(g);
-    if (dim == 2) compute_lsq(g);
     return gp.release();
 }
 
-// psstLeastSquare::initialize (psstGradCalculation.cpp:191-260), 2D. r_ is
+// psstLeastSquare::initialize (psstGradCalculation.cpp:191-260). r_ is
 // indexed by the cell's position inside its zone, so with several interior
 // zones the last zone (ascending id) with more than i cells wins; calculate()
-// reads it back the same way (:404-412).
-void compute_lsq(psst_grid &g) {
+// reads it back the same way (:404-412). kLsqNR coefficients per index: r11,
+// r12, r22 and, in 3D, r13, r23, r33 and beta, the Gram-Schmidt factors of the
+// weighted (w = 1/|dx|^2) normal equations as the reference forms them.
+std::vector<double> lsq_table(const psst_grid &g) {
+    const int dim = g.dim;
     int64_t maxc = 0;
     for (auto &z : g.vz)
         if (z.bc == 1) maxc = std::max(maxc, z.count);
-    g.lsq_r.assign(3 * (maxc + 1), 0.0);
+    std::vector<double> lsq_r(kLsqNR * (maxc + 1), 0.0);
     for (auto &z : g.vz) {
         if (z.bc != 1) continue;
         for (int64_t i = 0; i < z.count; ++i) {
             const int64_t v = z.first + i;
-            double ca = 0.0, cb = 0.0, cd = 0.0;
+            double ca = 0.0, cb = 0.0, cd = 0.0, cc = 0.0, ce = 0.0, cg = 0.0;
             for (int64_t e = g.vf_ptr[v]; e < g.vf_ptr[v + 1]; ++e) {
                 const int64_t f = g.vf_idx[e];
                 const int64_t nb = g.f_c0[f] == v ? g.f_c1[f] : g.f_c0[f];
-                double diff[2], w = 0.0;
-                for (int k = 0; k < 2; ++k) {
-                    diff[k] = g.xc[nb * 2 + k] - g.xc[v * 2 + k];
+                double diff[3] = {0.0, 0.0, 0.0}, w = 0.0;
+                for (int k = 0; k < dim; ++k) {
+                    diff[k] = g.xc[nb * dim + k] - g.xc[v * dim + k];
                     w += diff[k] * diff[k];
                 }
                 const double ws = 1.0 / w;
                 ca += ws * diff[0] * diff[0];
                 cb += ws * diff[0] * diff[1];
                 cd += ws * diff[1] * diff[1];
+                if (dim == 3) {
+                    cc += ws * diff[0] * diff[2];
+                    ce += ws * diff[1] * diff[2];
+                    cg += ws * diff[2] * diff[2];
+                }
             }
-            double *r = &g.lsq_r[3 * i];
+            double *r = &lsq_r[kLsqNR * i];
             r[0] = std::sqrt(ca);
             r[1] = cb / r[0];
             r[2] = std::sqrt(cd - r[1] * r[1]);
+            if (dim == 3) {
+                r[3] = cc / r[0];
+                r[4] = (ce - r[1] / r[0] * cc) / r[2];
+                r[5] = std::sqrt(cg - (r[3] * r[3] + r[4] * r[4]));
+                r[6] = (r[1] * r[4] - r[3] * r[2]) / (r[0] * r[2]);
+            }
         }
     }
+    return lsq_r;
 }
 
 }  // namespace psst

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -74,7 +75,6 @@ struct psst_grid {
     std::vector<int64_t> f_c0, f_c1;     // nface, volume index or -1
     std::vector<int32_t> f_fz;           // face -> fz slot
     std::vector<double> S, n, xf, beta;  // nface, nface*dim, nface*dim, nface
-    std::vector<double> lsq_r;           // 3 per zone-local interior index (2D least squares)
     double min_vol = -1.0;
     int max_faces = 0;
     // initial state holder filled by psst_case_read (SoA p,T,u..)
@@ -89,6 +89,13 @@ struct psst_grid {
 };
 
 namespace psst {
+// Runs fn(begin, end) over [0, n) split into contiguous chunks on the host
+// threads (PSST_HOST_THREADS, default: the hardware threads); small ranges run
+// inline. If chunks throw, the exception of the lowest failing chunk is
+// rethrown after all have finished, which is the first error a sequential
+// loop over [0, n) would have raised.
+void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)> &fn);
 psst_grid *build_grid(const RawMesh &m);
-void compute_lsq(psst_grid &g);
+constexpr int kLsqNR = 7;  // least-squares coefficients per cell: r11 r12 r22 (2D), + r13 r23 r33 beta (3D)
+std::vector<double> lsq_table(const psst_grid &g);  // kLsqNR per zone-local interior index
 }  // namespace psst

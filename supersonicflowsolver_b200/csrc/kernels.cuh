@@ -45,7 +45,41 @@ __device__ __forceinline__ void flag_error(int32_t *err, int code, int id) {
     if (atomicCAS(&err[0], 0, code) == 0) err[1] = id;
 }
 
-// 128-bit loads of a 16-byte-aligned record.
+// Record loads and stores. Record arrays start on cudaMalloc boundaries, so a
+// record whose size is a multiple of 32 bytes is 32-byte aligned and moves
+// with 256-bit accesses (sm_100 ld/st.global.v8.b32: one L1 request per
+// record instead of two for the 32-byte cell records and face outputs);
+// other records with 128-bit ones.
+//
+// ldg: for records the running kernel does not write (the asm has no memory
+// dependence, so the compiler may schedule it freely).
+template <typename T>
+__device__ __forceinline__ T ldg(const T *p) {
+    static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
+    union U {
+        T t;
+        uint32_t w[sizeof(T) / 4];
+        int4 v[sizeof(T) / 16];
+        __device__ U() {}
+    } u;
+    if constexpr (sizeof(T) % 32 == 0) {
+        const char *q = reinterpret_cast<const char *>(p);
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(T) / 32); ++i)
+            asm("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=r"(u.w[8 * i]), "=r"(u.w[8 * i + 1]), "=r"(u.w[8 * i + 2]), "=r"(u.w[8 * i + 3]),
+                  "=r"(u.w[8 * i + 4]), "=r"(u.w[8 * i + 5]), "=r"(u.w[8 * i + 6]), "=r"(u.w[8 * i + 7])
+                : "l"(q + 32 * i));
+    } else {
+        const int4 *q = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(T) / 16); ++i) u.v[i] = q[i];
+    }
+    return u.t;
+}
+
+// ld16: plain 128-bit loads, for records that other threads of the same
+// kernel may have written before a barrier (sequential LocalAccTime1).
 template <typename T>
 __device__ __forceinline__ T ld16(const T *p) {
     static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
@@ -64,13 +98,24 @@ __device__ __forceinline__ void st16(T *p, const T &t) {
     static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
     union U {
         T t;
+        uint32_t w[sizeof(T) / 4];
         int4 v[sizeof(T) / 16];
         __device__ U() {}
     } u;
     u.t = t;
-    int4 *q = reinterpret_cast<int4 *>(p);
+    if constexpr (sizeof(T) % 32 == 0) {
+        char *q = reinterpret_cast<char *>(p);
 #pragma unroll
-    for (int i = 0; i < (int)(sizeof(T) / 16); ++i) q[i] = u.v[i];
+        for (int i = 0; i < (int)(sizeof(T) / 32); ++i)
+            asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(q + 32 * i), "r"(u.w[8 * i]),
+                         "r"(u.w[8 * i + 1]), "r"(u.w[8 * i + 2]), "r"(u.w[8 * i + 3]), "r"(u.w[8 * i + 4]),
+                         "r"(u.w[8 * i + 5]), "r"(u.w[8 * i + 6]), "r"(u.w[8 * i + 7])
+                         : "memory");
+    } else {
+        int4 *q = reinterpret_cast<int4 *>(p);
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(T) / 16); ++i) q[i] = u.v[i];
+    }
 }
 
 // psstScalarLimiters.cpp:17-93
@@ -343,20 +388,20 @@ __global__ void __maxnreg__(PSST_FACE_MAXNREG) k_face(DevGrid g, DevState<R> st,
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
     if (g.face_case && !g.case_active[g.face_case[f]]) return;  // stopped case (merged grids)
-    const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
+    const FaceRec<R, DIM> fr = ldg(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
     R nn[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) nn[k] = (R)fr.n[k];
     const R S = (R)fr.S;
-    const Prim<R, DIM> p0 = unpack<R, DIM>(ld16(st.rec + fr.c0));
-    const Prim<R, DIM> p1 = unpack<R, DIM>(ld16(st.rec + fr.c1));
+    const Prim<R, DIM> p0 = unpack<R, DIM>(ldg(st.rec + fr.c0));
+    const Prim<R, DIM> p1 = unpack<R, DIM>(ldg(st.rec + fr.c1));
     R flow[DIM + 2];
     if (f < g.nfi) {
         const GradRec<R, DIM> *grec = reinterpret_cast<const GradRec<R, DIM> *>(wk.grec);
         GradRec<R, DIM> g0, g1;
         if (REC) {
-            g0 = ld16(grec + fr.c0);
-            g1 = ld16(grec + fr.c1);
+            g0 = ldg(grec + fr.c0);
+            g1 = ldg(grec + fr.c1);
         }
         Prim<R, DIM> r[2] = {p0, p1};
         if (!interior_flux<R, DIM, FLUX, REC, LIM>(r, &g0, &g1, fr, nn, gas, flow)) {
@@ -405,8 +450,11 @@ __global__ void __maxnreg__(PSST_FACE_MAXNREG) k_face(DevGrid g, DevState<R> st,
 // Thread per cell. psstGreenGauss::calculate (psstGradCalculation.cpp:80-177)
 // as a per-cell gather: grad_c += sign * (beta*phi0 + (1-beta)*phi1) * S/V_c * n,
 // sign -1 on side 0, +1 on side 1, faces in the reference's loop order; or the
-// 2D least squares of psstLeastSquare::calculate (:268-368) in the cell's own
-// face order. Then, for limiters 4/5, the Barth-Jespersen (AIAA 89-0366) /
+// least squares of psstLeastSquare::calculate (:268-368) in the cell's own
+// face order: 2D as the reference; 3D as a corrected restatement (the
+// reference's 3D branch leaves alpha_1, alpha_2 at zero and writes alpha[3]
+// out of bounds, :338): alpha_3 = (dz - r23/r22 dy + beta dx) / r33^2
+// (Anderson & Bonhaus 1994), then the reference's theta corrections. Then, for limiters 4/5, the Barth-Jespersen (AIAA 89-0366) /
 // Venkatakrishnan (AIAA 93-0880) cell limiter:
 // psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c).
 template <typename R, int DIM, int GRAD, int CELLLIM>
@@ -417,7 +465,7 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
     if (g.cell_case && !g.case_active[g.cell_case[c]]) return;  // stopped case
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
-    const Prim<R, DIM> own = unpack<R, DIM>(ld16(st.rec + c));
+    const Prim<R, DIM> own = unpack<R, DIM>(ldg(st.rec + c));
     R gr[NVAR][DIM];
 #pragma unroll
     for (int i = 0; i < NVAR; ++i)
@@ -434,8 +482,8 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
         for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
             const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
-            const FaceRec<R, DIM> fr = ld16(frec + f);
-            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + g.csr_nb[b + q]));
+            const FaceRec<R, DIM> fr = ldg(frec + f);
+            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + g.csr_nb[b + q]));
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -457,12 +505,16 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
             }
         }
     } else {
-        const R r0 = (R)g.lsq_r[c], r1 = (R)g.lsq_r[(int64_t)g.nint + c], r2 = (R)g.lsq_r[2 * (int64_t)g.nint + c];
-        const R xc0 = (R)g.xc[c], xc1 = (R)g.xc[(int64_t)g.nall + c];
+        constexpr int NR = DIM == 2 ? 3 : 7;  // r11 r12 r22 (r13 r23 r33 beta)
+        R r[NR], xo[DIM];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) r[q] = (R)g.lsq_r[(int64_t)q * g.nint + c];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) xo[k] = (R)g.xc[(int64_t)k * g.nall + c];
         for (int32_t j = 0; j < K; ++j) {
             const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
             const int32_t nb = g.csr_nb[slot];
-            const Prim<R, DIM> oth = unpack<R, DIM>(ld16(st.rec + nb));
+            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + nb));
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -470,21 +522,30 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
                     if (v > mx[i]) mx[i] = v;
                     if (v < mn[i]) mn[i] = v;
                 }
-            R diff[2];
-            diff[0] = (R)g.xc[nb] - xc0;
-            diff[1] = (R)g.xc[(int64_t)g.nall + nb] - xc1;
+            R diff[DIM];
             R w = (R)0;
-            w += diff[0] * diff[0];
-            w += diff[1] * diff[1];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                diff[k] = (R)g.xc[(int64_t)k * g.nall + nb] - xo[k];
+                w += diff[k] * diff[k];
+            }
             const R ws = (R)1 / w;
-            const R al0 = diff[0] / (r0 * r0);
-            const R al1 = (diff[1] - r1 / r0 * diff[0]) / (r2 * r2);
-            const R th[2] = {al0 - r1 / r0 * al1, al1};
+            const R al0 = diff[0] / (r[0] * r[0]);
+            const R al1 = (diff[1] - r[1] / r[0] * diff[0]) / (r[2] * r[2]);
+            R th[DIM];
+            th[0] = al0 - r[1] / r[0] * al1;
+            th[1] = al1;
+            if constexpr (DIM == 3) {  // corrected 3D restatement (see above)
+                const R al2 = (diff[2] - r[4] / r[2] * diff[1] + r[6] * diff[0]) / (r[5] * r[5]);
+                th[0] += al2 * r[6];
+                th[1] -= r[4] / r[2] * al2;
+                th[2] = al2;
+            }
 #pragma unroll
             for (int i = 0; i < NVAR; ++i) {
                 const R phi = (pvar<R, DIM>(oth, i) - pvar<R, DIM>(own, i));
 #pragma unroll
-                for (int k = 0; k < 2; ++k) gr[i][k] += ws * th[k] * phi;
+                for (int k = 0; k < DIM; ++k) gr[i][k] += ws * th[k] * phi;
             }
         }
     }
@@ -499,7 +560,7 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
-            const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
+            const FaceRec<R, DIM> fr = ldg(frec + (ent >> 1));
             R off[DIM];  // x_f - x_c of this cell
 #pragma unroll
             for (int k = 0; k < DIM; ++k) off[k] = (ent & 1) ? fr.o1[k] : fr.o0[k];
@@ -658,7 +719,7 @@ __device__ __forceinline__ CellRec<R> ghost_state(const DevGrid &g, const CellRe
         for (int k = 0; k < DIM; ++k) s.u[k] = nb.u[k];
         s.p = nb.p;
     } else if (dyn == 15) {
-        const FaceRec<R, DIM> fr = ld16(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + g.g_face[i]);
+        const FaceRec<R, DIM> fr = ldg(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + g.g_face[i]);
         R vn = (R)0;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) vn += nb.u[k] * (R)fr.n[k];
@@ -808,7 +869,7 @@ __device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<
     for (int v = 0; v < DIM + 2; ++v) res[v] = (R)0;
     for (int32_t q = g.csr_ptr[c]; q < g.csr_ptr[c + 1]; ++q) {
         const int32_t ent = g.csr_ent[q];
-        const FaceOut<R, DIM> o = ld16(fo + (ent >> 1));
+        const FaceOut<R, DIM> o = ldg(fo + (ent >> 1));
         if (ent & 1) {
 #pragma unroll
             for (int v = 0; v < DIM + 2; ++v) res[v] += o.v[v];
@@ -863,8 +924,8 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
     bool run = c < g.nint;
     if (BATCH && run && !g.case_active[g.cell_case[c]]) {  // stopped case: carry the state over
         run = false;
-        st16(nxt.rec + c, ld16(cur.rec + c));
-        for (int32_t i = g.gptr[c]; i < g.gptr[c + 1]; ++i) st16(nxt.rec + g.nint + i, ld16(cur.rec + g.nint + i));
+        st16(nxt.rec + c, ldg(cur.rec + c));
+        for (int32_t i = g.gptr[c]; i < g.gptr[c + 1]; ++i) st16(nxt.rec + g.nint + i, ldg(cur.rec + g.nint + i));
     }
     if (run) {
         const FO *fo = reinterpret_cast<const FO *>(wk.fout);
@@ -885,7 +946,7 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
 #pragma unroll 4
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
-            const FO o = ld16(fo + (ent >> 1));
+            const FO o = ldg(fo + (ent >> 1));
             const int side = ent & 1;
             if (side) {
 #pragma unroll
@@ -911,7 +972,7 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
                 for (int32_t j = 0; j < K; ++j) {
                     const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
                     const int32_t ent = g.csr_ent[slot];
-                    const FO o = ld16(fo + (ent >> 1));
+                    const FO o = ldg(fo + (ent >> 1));
                     const int side = ent & 1;
                     const R nv = lc1_normal_velocities<R, DIM>(o, side, nnb);
                     nnb = (nnb + nv) * (R)0.5;
@@ -921,11 +982,11 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
                 if (!one_pass)
                     for (int32_t j = 0; j < K; ++j) {
                         const int32_t ent = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
-                        const FO o = ld16(fo + (ent >> 1));
+                        const FO o = ldg(fo + (ent >> 1));
 #pragma unroll
                         for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
                     }
-                const Prim<R, DIM> own = unpack<R, DIM>(ld16(cur.rec + c));
+                const Prim<R, DIM> own = unpack<R, DIM>(ldg(cur.rec + c));
                 const R cc = sqrt((R)gas.gamma * (R)gas.rm * own.T);
 #pragma unroll
                 for (int k = 0; k < DIM; ++k) den += (fabs(own.u[k]) + cc) * s[k] * (R)0.5;
@@ -940,7 +1001,7 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
             const Prim<R, DIM> np = unpack<R, DIM>(nrec);
             for (int32_t i = g0; i < g1; ++i) {
                 const int32_t gc = g.nint + i;
-                st16(nxt.rec + gc, ghost_state<R, DIM>(g, ld16(cur.rec + gc), np, i, gas));
+                st16(nxt.rec + gc, ghost_state<R, DIM>(g, ldg(cur.rec + gc), np, i, gas));
             }
         }
     }
@@ -966,7 +1027,7 @@ __device__ __forceinline__ void update_from_buffers(const DevGrid &g, const DevS
 #pragma unroll
         for (int v = 0; v < NV; ++v) res[v] = wk.res[(int64_t)v * g.nint + c];
     }
-    const Prim<R, DIM> own = unpack<R, DIM>(ld16(cur.rec + c));
+    const Prim<R, DIM> own = unpack<R, DIM>(ldg(cur.rec + c));
     double dt;
     if (seq)
         dt = local_time<R, DIM, 1, true>(g, cur.rec, nxt.rec, gas, cfl, dt_uniform, c, own);

@@ -67,13 +67,13 @@ static void gradient_dim(int grad, int celllim, const DevGrid &g, const DevState
             k_gradient<R, DIM, 1, 5><<<nb, bs, 0, s>>>(g, st, wk);
         else
             k_gradient<R, DIM, 1, 0><<<nb, bs, 0, s>>>(g, st, wk);
-    } else if (DIM == 2) {
+    } else {
         if (celllim == 4)
-            k_gradient<R, 2, 2, 4><<<nb, bs, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 2, 4><<<nb, bs, 0, s>>>(g, st, wk);
         else if (celllim == 5)
-            k_gradient<R, 2, 2, 5><<<nb, bs, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 2, 5><<<nb, bs, 0, s>>>(g, st, wk);
         else
-            k_gradient<R, 2, 2, 0><<<nb, bs, 0, s>>>(g, st, wk);
+            k_gradient<R, DIM, 2, 0><<<nb, bs, 0, s>>>(g, st, wk);
     }
 }
 

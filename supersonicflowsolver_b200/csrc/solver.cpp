@@ -267,15 +267,20 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         L.z_p.push_back(0);
         L.z_T.push_back(0);
     }
-    // 2D least squares: r_ table indexed by the zone-local position
-    // (psstGradCalculation.cpp:404-412)
-    L.lsq_r.assign((size_t)3 * L.nint, 0.0);
-    if (dim == 2 && !G.lsq_r.empty())
+    // least squares: r_ table indexed by the zone-local position
+    // (psstGradCalculation.cpp:404-412), one device array per coefficient
+    const int nr = dim == 2 ? 3 : kLsqNR;
+    if (sc.order == 2 && sc.grad == 2) {
+        const std::vector<double> tab = lsq_table(G);
+        L.lsq_r.assign((size_t)nr * L.nint, 0.0);
         for (int32_t d = 0; d < L.nint; ++d) {
             const int64_t v = L.vol_of_dev[d];
             const int64_t i = v - G.vz[G.vol_vz[v]].first;
-            for (int q = 0; q < 3; ++q) L.lsq_r[(size_t)q * L.nint + d] = G.lsq_r[3 * i + q];
+            for (int q = 0; q < nr; ++q) L.lsq_r[(size_t)q * L.nint + d] = tab[kLsqNR * i + q];
         }
+    } else {
+        L.lsq_r.assign(1, 0.0);
+    }
     L.vk_eps2.assign(L.nint, 0.0);
     for (int32_t d = 0; d < L.nint; ++d) {
         const double h = dim == 2 ? std::sqrt(L.V[d]) : std::cbrt(L.V[d]);
@@ -879,9 +884,6 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
         raise(PSST_ERR_ARG, "second order needs a limiter (1 VanAlbada, 2 MinMod, 3 VanLeer, 4 BJ, 5 Venkatakrishnan)");
     if (sc->lc < 0 || sc->lc > 2) raise(PSST_ERR_ARG, "unknown local time step mode");
     if (sc->rk_level < 1 || sc->rk_level > 16) raise(PSST_ERR_ARG, "Error: Unknow RK order!");
-    if (sc->order == 2 && sc->grad != 1 && G->dim != 2)
-        raise(PSST_ERR_UNSUPPORTED, "least-squares gradient: the reference's 3D path writes out of bounds "
-                                    "(psstGradCalculation.cpp:338); only 2D is supported");
     if (sc->order == 2 && sc->grad != 1 && G->case_vol_ptr.size() > 2)
         raise(PSST_ERR_UNSUPPORTED, "merged grids need Green-Gauss gradients (the least-squares table is "
                                     "indexed across zones, psstGradCalculation.cpp:404-412)");

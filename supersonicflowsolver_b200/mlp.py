@@ -62,15 +62,25 @@ class MLP:
         p = np.ascontiguousarray(p, dtype=np.float32)
         check(_lib.load().psst_mlp_set_params(self._h, p.ctypes.data, self.n))
 
+    def _on_torch_stream(self):
+        """The network's kernels run on torch's current stream, in order with
+        the kernels that made the input tensors and before any that read the
+        outputs (the library's own stream would race with both)."""
+        import torch
+
+        self.set_stream(torch.cuda.current_stream().cuda_stream)
+
     def forward(self, x):
         """x: torch CUDA FP32 [B][4] -> torch CUDA FP32 [B][4]."""
         import torch
 
+        self._on_torch_stream()
         y = torch.empty((x.shape[0], 4), dtype=torch.float32, device=x.device)
         check(_lib.load().psst_mlp_forward(self._h, x.data_ptr(), int(x.shape[0]), y.data_ptr()))
         return y
 
     def gradients(self, x, t):
+        self._on_torch_stream()
         g = np.zeros(self.n, dtype=np.float32)
         loss = ctypes.c_float()
         check(_lib.load().psst_mlp_gradients(self._h, x.data_ptr(), t.data_ptr(), int(x.shape[0]), g.ctypes.data,
@@ -78,6 +88,7 @@ class MLP:
         return g, loss.value
 
     def train_step(self, x, t, lr):
+        self._on_torch_stream()
         loss = ctypes.c_float()
         check(_lib.load().psst_mlp_train_step(self._h, x.data_ptr(), t.data_ptr(), int(x.shape[0]), float(lr),
                                                ctypes.byref(loss)))

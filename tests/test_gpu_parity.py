@@ -50,6 +50,9 @@ CASES = [
     ("2d_adapted_hllc_vanleer", "a", dict(flux=3, order=2, limiter=3, lc=1), 4),
     ("2d_adapted_ausm_lsq_vanalbada_lc2", "a", dict(flux=1, order=2, limiter=1, lc=2, grad=2), 4),
     ("2d_adapted_hllc_bj", "a", dict(flux=3, order=2, limiter=4, lc=1), 4),
+    # 3D least squares: corrected restatement (no reference counterpart)
+    ("3d_tets_hllc_lsq_vanleer", "t", dict(flux=3, order=2, limiter=3, lc=1, grad=2, mach=3.0), 3),
+    ("3d_hexes_ausm_lsq_venkat_lc2", "h", dict(flux=1, order=2, limiter=5, lc=2, grad=2, mach=3.0), 3),
 ]
 MESH = {
     "q": lambda: meshgen.wedge2d(30, 10, 15.0),

@@ -102,6 +102,28 @@ def test_oracle_matches_reference_on_its_adapted_samples(tmp_path, mesh):
     _check_vs_reference_files(str(tmp_path / "m.msh"), str(tmp_path), "c", 4)
 
 
+@pytest.mark.parametrize("tets", [True, False], ids=["tets", "hexes"])
+def test_oracle_3d_least_squares_exact_for_linear_fields(tmp_path, tets):
+    """The 3D least-squares gradient (corrected restatement: the reference's
+    3D branch writes out of bounds) reproduces linear fields to rounding at
+    every interior cell, ghosts holding the same field at their face centres."""
+    mesh = meshgen.wedge3d(8, 4, 3, 12.0, tets=tets)
+    path, d, name = make_case(tmp_path, mesh, max_iter=1, flux=3, order=2, limiter=3, lc=1, grad=2, mach=3.0)
+    o = Oracle(path, d, name)
+    x = o.get("vol_x").reshape(-1, 3)
+    gp, gT = np.array([3.0e3, -2.0e3, 0.5e3]), np.array([10.0, 40.0, -15.0])
+    gu = np.array([[5.0, 10.0, 15.0], [20.0, 0.0, 0.0], [0.0, 0.0, -7.0]])
+    u = np.array([800.0, 0.0, 0.0]) + x @ gu.T
+    o.set_prim(101325.0 + x @ gp, 300.0 + x @ gT, u.ravel())
+    o.run(1)
+    inner = o.get("vol_bc") == 1
+    for key, ref in (("vol_grad_p", gp), ("vol_grad_T", gT)):
+        got = o.get(key).reshape(-1, 3)[inner]
+        assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref)) * 100, key
+    gotu = o.get("vol_grad_u").reshape(-1, 3, 3)[inner]
+    assert np.max(np.abs(gotu - gu)) <= 1e-10
+
+
 def _check_vs_reference(tmp_path, mesh, ckw, n):
     path, d, name = make_case(tmp_path, mesh, max_iter=n, **ckw)
     _check_vs_reference_files(path, d, name, n)
