@@ -164,24 +164,24 @@ void green_gauss_beta(psst_grid &g) {
     for (auto &z : g.fz) {
         if (z.bc == 31) continue;
         parallel_for(z.count, [&](int64_t i0, int64_t i1) {
-        for (int64_t i = i0; i < i1; ++i) {
-            const int64_t f = z.first + i;
-            double d[2];
-            for (int j = 0; j < 2; ++j) {
-                d[j] = 0.0;
-                const int64_t v = j == 0 ? g.f_c0[f] : g.f_c1[f];
-                if (v >= 0 && !g.vol_boundary[v]) {
-                    double dist = 0.0;
-                    for (int k = 0; k < dim; ++k) {
-                        double add = (g.xf[f * dim + k] - g.xc[v * dim + k]);
-                        add = add * add;
-                        dist += add;
+            for (int64_t i = i0; i < i1; ++i) {
+                const int64_t f = z.first + i;
+                double d[2];
+                for (int j = 0; j < 2; ++j) {
+                    d[j] = 0.0;
+                    const int64_t v = j == 0 ? g.f_c0[f] : g.f_c1[f];
+                    if (v >= 0 && !g.vol_boundary[v]) {
+                        double dist = 0.0;
+                        for (int k = 0; k < dim; ++k) {
+                            double add = (g.xf[f * dim + k] - g.xc[v * dim + k]);
+                            add = add * add;
+                            dist += add;
+                        }
+                        d[j] = std::sqrt(dist);
                     }
-                    d[j] = std::sqrt(dist);
                 }
+                bz[i] = d[1] / (d[0] + d[1]);
             }
-            bz[i] = d[1] / (d[0] + d[1]);
-        }
         });
     }
     for (auto &z : g.fz)

@@ -5,6 +5,7 @@
 // as flat arrays, plus everything the device layout is derived from.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <functional>
 #include <memory>
@@ -95,6 +96,35 @@ namespace psst {
 // rethrown after all have finished, which is the first error a sequential
 // loop over [0, n) would have raised.
 void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)> &fn);
+int host_threads();
+// Runs fn(t) for t in [0, ntasks), each task on its own host thread.
+void parallel_tasks(int ntasks, const std::function<void(int)> &fn);
+
+// Sorts v by cmp, a strict total order (make keys unique, e.g. by an index,
+// so that the result equals a stable sort): chunks sorted in parallel, then
+// merged pairwise in parallel.
+template <class T, class Cmp>
+void parallel_sort(std::vector<T> &v, Cmp cmp) {
+    const int64_t n = (int64_t)v.size();
+    int chunks = 1;
+    while (chunks * 2 <= host_threads() && n / (chunks * 2) >= 65536) chunks *= 2;
+    if (chunks == 1) {
+        std::sort(v.begin(), v.end(), cmp);
+        return;
+    }
+    std::vector<int64_t> cut((size_t)chunks + 1);
+    for (int i = 0; i <= chunks; ++i) cut[(size_t)i] = n * i / chunks;
+    parallel_tasks(chunks, [&](int t) { std::sort(v.begin() + cut[(size_t)t], v.begin() + cut[(size_t)t + 1], cmp); });
+    std::vector<T> tmp((size_t)n);
+    for (int width = 1; width < chunks; width *= 2) {
+        parallel_tasks(chunks / (2 * width), [&](int p) {
+            const int64_t a = cut[(size_t)(2 * p * width)], m = cut[(size_t)((2 * p + 1) * width)],
+                          b = cut[(size_t)((2 * p + 2) * width)];
+            std::merge(v.begin() + a, v.begin() + m, v.begin() + m, v.begin() + b, tmp.begin() + a, cmp);
+        });
+        v.swap(tmp);
+    }
+}
 psst_grid *build_grid(const RawMesh &m);
 constexpr int kLsqNR = 7;  // least-squares coefficients per cell: r11 r12 r22 (2D), + r13 r23 r33 beta (3D)
 std::vector<double> lsq_table(const psst_grid &g);  // kLsqNR per zone-local interior index

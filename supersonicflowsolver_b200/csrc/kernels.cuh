@@ -674,14 +674,18 @@ __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<
                                                 bool keep, int32_t c, const R res[DIM + 2], double sq[DIM + 2],
                                                 double mx[DIM + 2]) {
     constexpr int NV = DIM + 2;
+    // FP64 (parity) path: the reference's operation order, one division per
+    // component; FP32 path: one reciprocal per cell (its own rounding)
+    constexpr bool EXACT = sizeof(R) == 8;
     const double vol = in.vol;
+    const double step = EXACT ? 0.0 : dt * alpha / vol;
     double w[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const int64_t idx = (int64_t)v * g.nint + c;
         const double pw = in.pw[v];
         if (first_stage) wk.pw[idx] = pw;
-        w[v] = pw - dt * alpha * (double)res[v] / vol;
+        w[v] = EXACT ? pw - dt * alpha * (double)res[v] / vol : pw - step * (double)res[v];
         if (keep) wk.w[idx] = w[v];
         const double rv = (double)res[v];
         const double ar = fabs(rv);
@@ -690,15 +694,17 @@ __device__ __forceinline__ CellRec<R> rk_update(const DevGrid &g, const DevWork<
         if (!(rv - rv == 0.0)) flag_error(wk.err, ERR_NONFINITE_RES, c);
     }
     const double rho = w[DIM];
+    const double irho = EXACT ? 0.0 : 1.0 / rho;
     double vs = 0.0;
     R u[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        const double uk = w[k] / rho;
+        const double uk = EXACT ? w[k] / rho : w[k] * irho;
         u[k] = (R)uk;
         vs += uk * uk;
     }
-    const double T = ((w[DIM + 1] / rho) - (vs * 0.5)) / gas.cv;
+    const double T = EXACT ? ((w[DIM + 1] / rho) - (vs * 0.5)) / gas.cv
+                           : ((w[DIM + 1] * irho) - (vs * 0.5)) * (1.0 / gas.cv);
     const double p = rho * gas.rm * T;
     if (!(rho > 0.0 && T > 0.0)) flag_error(wk.err, ERR_BAD_STATE, c);
     if (keep) wk.dt[c] = dt;
@@ -736,18 +742,25 @@ __device__ __forceinline__ CellRec<R> ghost_state(const DevGrid &g, const CellRe
 
 // Block partials of the residual norms: part[block][v] = sum res^2,
 // part[block][NV + v] = max |res|; fixed reduction pattern (reproducible).
-template <int NV>
+// FMAX: the maxima are FP32 values (FP32 residuals), reduced as floats
+// (exact: a max selects one of its inputs).
+template <int NV, bool FMAX = false>
 __device__ __forceinline__ void block_norm_partials(double sq[NV], double mx[NV], double *part) {
     __shared__ double red[2 * NV][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         double x = sq[v], m = mx[v];
+        float mf = (float)m;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             x += __shfl_down_sync(FULL, x, o);
-            m = fmax(m, __shfl_down_sync(FULL, m, o));
+            if (FMAX)
+                mf = fmaxf(mf, __shfl_down_sync(FULL, mf, o));
+            else
+                m = fmax(m, __shfl_down_sync(FULL, m, o));
         }
+        if (FMAX) m = (double)mf;
         if (lane == 0) {
             red[v][wid] = x;
             red[NV + v][wid] = m;
@@ -1006,7 +1019,7 @@ __global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevStat
         }
     }
     if (BATCH) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, run ? g.cell_case[c] : -1, mx);
-    block_norm_partials<NV>(sq, mx, wk.l2part);
+    block_norm_partials<NV, sizeof(R) == 4>(sq, mx, wk.l2part);
     last_block_finish<NV>(wk.l2part, wk.ticket, g.nint, wk.linf, wk.l2, it_slot);
 }
 

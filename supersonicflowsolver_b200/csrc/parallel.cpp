@@ -8,7 +8,6 @@
 
 namespace psst {
 
-namespace {
 int host_threads() {
     static const int n = [] {
         const char *e = std::getenv("PSST_HOST_THREADS");
@@ -17,7 +16,23 @@ int host_threads() {
     }();
     return n;
 }
-}  // namespace
+
+void parallel_tasks(int ntasks, const std::function<void(int)> &fn) {
+    std::vector<std::exception_ptr> err((size_t)std::max(ntasks, 0));
+    std::vector<std::thread> pool;
+    auto run = [&](int t) {
+        try {
+            fn(t);
+        } catch (...) {
+            err[(size_t)t] = std::current_exception();
+        }
+    };
+    for (int t = 1; t < ntasks; ++t) pool.emplace_back(run, t);
+    if (ntasks > 0) run(0);
+    for (auto &th : pool) th.join();
+    for (auto &e : err)
+        if (e) std::rethrow_exception(e);
+}
 
 void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)> &fn) {
     constexpr int64_t kMinChunk = 16384;

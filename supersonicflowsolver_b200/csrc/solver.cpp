@@ -104,29 +104,35 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
             }
         const int bits = dim == 3 ? 21 : 31;
         const double scale = (double)((1u << bits) - 1);
-        std::vector<uint64_t> key(L.nint);
-        for (int32_t i = 0; i < L.nint; ++i) {
-            uint32_t X[3] = {0, 0, 0};
-            for (int k = 0; k < dim; ++k) {
-                const double span = hi[k] - lo[k];
-                const double t = span > 0 ? (G.xc[ref_int[i] * dim + k] - lo[k]) / span : 0.0;
-                X[k] = (uint32_t)std::min(scale, std::max(0.0, t * scale));
+        // (case, Hilbert key, reference position): sorting these orders each
+        // case contiguously (merged grids), Hilbert order inside it, ties in
+        // reference order
+        struct Key {
+            int64_t cs;
+            uint64_t key;
+            int64_t i;
+            bool operator<(const Key &o) const {
+                return cs != o.cs ? cs < o.cs : key != o.key ? key < o.key : i < o.i;
             }
-            key[i] = hilbert_key(X, bits, dim);
-        }
-        if (G.case_vol_ptr.empty()) {
-            std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
-        } else {  // merged grid: each case stays contiguous, Hilbert order inside it
-            auto cs = [&](int64_t i) {
-                return std::upper_bound(G.case_vol_ptr.begin(), G.case_vol_ptr.end(), ref_int[i]) -
-                       G.case_vol_ptr.begin();
-            };
-            std::vector<int64_t> icase(L.nint);
-            for (int32_t i = 0; i < L.nint; ++i) icase[i] = cs(i);
-            std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-                return icase[a] != icase[b] ? icase[a] < icase[b] : key[a] < key[b];
-            });
-        }
+        };
+        std::vector<Key> keys(L.nint);
+        parallel_for(L.nint, [&](int64_t i0, int64_t i1) {
+            for (int64_t i = i0; i < i1; ++i) {
+                uint32_t X[3] = {0, 0, 0};
+                for (int k = 0; k < dim; ++k) {
+                    const double span = hi[k] - lo[k];
+                    const double t = span > 0 ? (G.xc[ref_int[i] * dim + k] - lo[k]) / span : 0.0;
+                    X[k] = (uint32_t)std::min(scale, std::max(0.0, t * scale));
+                }
+                const int64_t cs = G.case_vol_ptr.empty()
+                                       ? 0
+                                       : std::upper_bound(G.case_vol_ptr.begin(), G.case_vol_ptr.end(), ref_int[i]) -
+                                             G.case_vol_ptr.begin();
+                keys[i] = Key{cs, hilbert_key(X, bits, dim), i};
+            }
+        });
+        parallel_sort(keys, [](const Key &a, const Key &b) { return a < b; });
+        for (int32_t i = 0; i < L.nint; ++i) order[i] = keys[i].i;
     }
     L.vol_of_dev.assign(L.nall, -1);
     L.rank.assign(L.nint, 0);
@@ -173,9 +179,21 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         if (!zone_interior && ga == gb) raise(PSST_ERR_FORMAT, "boundary face without exactly one ghost side");
         (zone_interior ? fint : fbnd).push_back(f);
     }
-    auto lowcell = [&](int64_t f) { return std::min(L.dev_of_vol[G.f_c0[f]], L.dev_of_vol[G.f_c1[f]]); };
-    std::stable_sort(fint.begin(), fint.end(), [&](int64_t a, int64_t b) { return lowcell(a) < lowcell(b); });
-    std::stable_sort(fbnd.begin(), fbnd.end(), [&](int64_t a, int64_t b) { return lowcell(a) < lowcell(b); });
+    // stable counting sort of each list by its lower device cell
+    auto by_lowcell = [&](std::vector<int64_t> &fs) {
+        std::vector<int64_t> start((size_t)L.nall + 1, 0);
+        std::vector<int32_t> low(fs.size());
+        for (size_t i = 0; i < fs.size(); ++i) {
+            low[i] = std::min(L.dev_of_vol[G.f_c0[fs[i]]], L.dev_of_vol[G.f_c1[fs[i]]]);
+            ++start[(size_t)low[i] + 1];
+        }
+        for (int32_t c = 0; c < L.nall; ++c) start[(size_t)c + 1] += start[(size_t)c];
+        std::vector<int64_t> out(fs.size());
+        for (size_t i = 0; i < fs.size(); ++i) out[(size_t)start[(size_t)low[i]]++] = fs[i];
+        fs.swap(out);
+    };
+    by_lowcell(fint);
+    by_lowcell(fbnd);
     L.nfi = (int32_t)fint.size();
     L.nface = (int32_t)(fint.size() + fbnd.size());
     std::vector<int32_t> dev_face(G.nface, -1);
@@ -189,25 +207,29 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
     L.beta.resize(L.nface);
     L.n.resize((size_t)dim * L.nface);
     L.xf.resize((size_t)dim * L.nface);
-    for (int32_t d = 0; d < L.nface; ++d) {
-        const int64_t f = ref_face[d];
-        L.c0[d] = L.dev_of_vol[G.f_c0[f]];
-        L.c1[d] = L.dev_of_vol[G.f_c1[f]];
-        L.S[d] = G.S[f];
-        L.beta[d] = G.beta[f];
-        for (int k = 0; k < dim; ++k) {
-            L.n[(size_t)k * L.nface + d] = G.n[f * dim + k];
-            L.xf[(size_t)k * L.nface + d] = G.xf[f * dim + k];
+    parallel_for(L.nface, [&](int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) {
+            const int64_t f = ref_face[d];
+            L.c0[d] = L.dev_of_vol[G.f_c0[f]];
+            L.c1[d] = L.dev_of_vol[G.f_c1[f]];
+            L.S[d] = G.S[f];
+            L.beta[d] = G.beta[f];
+            for (int k = 0; k < dim; ++k) {
+                L.n[(size_t)k * L.nface + d] = G.n[f * dim + k];
+                L.xf[(size_t)k * L.nface + d] = G.xf[f * dim + k];
+            }
         }
-    }
+    });
     // cells: volume, centroid, CSR sorted by reference face index (= loop order)
     L.V.resize(L.nint);
     L.xc.resize((size_t)dim * L.nall);
-    for (int32_t d = 0; d < L.nall; ++d) {
-        const int64_t v = L.vol_of_dev[d];
-        if (d < L.nint) L.V[d] = G.V[v];
-        for (int k = 0; k < dim; ++k) L.xc[(size_t)k * L.nall + d] = G.xc[v * dim + k];
-    }
+    parallel_for(L.nall, [&](int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) {
+            const int64_t v = L.vol_of_dev[d];
+            if (d < L.nint) L.V[d] = G.V[v];
+            for (int k = 0; k < dim; ++k) L.xc[(size_t)k * L.nall + d] = G.xc[v * dim + k];
+        }
+    });
     L.csr_ptr.assign(L.nint + 1, 0);
     L.wperm.assign(L.nint, 0);
     for (int32_t d = 0; d < L.nint; ++d) {
@@ -216,24 +238,25 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
     }
     L.csr_ent.resize(L.csr_ptr[L.nint]);
     L.csr_nb.resize(L.csr_ptr[L.nint]);
-    for (int32_t d = 0; d < L.nint; ++d) {
-        const int64_t v = L.vol_of_dev[d];
-        const int64_t b = G.vf_ptr[v], k = G.vf_ptr[v + 1] - b;
-        std::vector<int> idx(k);
-        std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return G.vf_idx[b + x] < G.vf_idx[b + y]; });
-        std::vector<int> pos(k);
-        for (int q = 0; q < k; ++q) {
-            const int64_t f = G.vf_idx[b + idx[q]];
-            const int side = G.f_c0[f] == v ? 0 : 1;
-            L.csr_ent[L.csr_ptr[d] + q] = (dev_face[f] << 1) | side;
-            L.csr_nb[L.csr_ptr[d] + q] = side ? L.c0[dev_face[f]] : L.c1[dev_face[f]];
-            pos[idx[q]] = q;
+    parallel_for(L.nint, [&](int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) {
+            const int64_t v = L.vol_of_dev[d];
+            const int64_t b = G.vf_ptr[v], k = G.vf_ptr[v + 1] - b;  // k <= 16 (checked above)
+            int idx[16], pos[16];
+            std::iota(idx, idx + k, 0);
+            std::stable_sort(idx, idx + k, [&](int x, int y) { return G.vf_idx[b + x] < G.vf_idx[b + y]; });
+            for (int q = 0; q < k; ++q) {
+                const int64_t f = G.vf_idx[b + idx[q]];
+                const int side = G.f_c0[f] == v ? 0 : 1;
+                L.csr_ent[L.csr_ptr[d] + q] = (dev_face[f] << 1) | side;
+                L.csr_nb[L.csr_ptr[d] + q] = side ? L.c0[dev_face[f]] : L.c1[dev_face[f]];
+                pos[idx[q]] = q;
+            }
+            uint64_t perm = 0;
+            for (int j = 0; j < k; ++j) perm |= (uint64_t)pos[j] << (4 * j);
+            L.wperm[d] = perm;
         }
-        uint64_t perm = 0;
-        for (int j = 0; j < k; ++j) perm |= (uint64_t)pos[j] << (4 * j);
-        L.wperm[d] = perm;
-    }
+    });
     // ghost tables and boundary zones; ghosts are sorted by interior neighbour,
     // so each interior cell owns a contiguous ghost range [gptr[d], gptr[d+1])
     L.g_nb.resize(L.nghost);
@@ -322,25 +345,27 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
 template <typename R, int DIM>
 std::vector<FaceRec<R, DIM>> build_face_records(const psst_grid &G, const Layout &L, int rec) {
     std::vector<FaceRec<R, DIM>> out(L.nface);
-    for (int32_t d = 0; d < L.nface; ++d) {
-        FaceRec<R, DIM> r;
-        std::memset(&r, 0, sizeof r);
-        r.c0 = L.c0[d];
-        r.c1 = L.c1[d];
-        r.S = L.S[d];
-        for (int k = 0; k < DIM; ++k) {
-            r.n[k] = L.n[(size_t)k * L.nface + d];
-            const double xf = L.xf[(size_t)k * L.nface + d];
-            const double x0 = L.xc[(size_t)k * L.nall + r.c0], x1 = L.xc[(size_t)k * L.nall + r.c1];
-            if (rec == 1) {  // Darwish-Moukalled: R = x_c0 - x_c1 (psstValueReconstructor.cpp:105-107)
-                r.o0[k] = (R)(x0 - x1);
-            } else if (rec == 2) {  // MUSCL: x_f - x_c per side
-                r.o0[k] = (R)(xf - x0);
-                r.o1[k] = (R)(xf - x1);
+    parallel_for(L.nface, [&](int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) {
+            FaceRec<R, DIM> r;
+            std::memset(&r, 0, sizeof r);
+            r.c0 = L.c0[d];
+            r.c1 = L.c1[d];
+            r.S = L.S[d];
+            for (int k = 0; k < DIM; ++k) {
+                r.n[k] = L.n[(size_t)k * L.nface + d];
+                const double xf = L.xf[(size_t)k * L.nface + d];
+                const double x0 = L.xc[(size_t)k * L.nall + r.c0], x1 = L.xc[(size_t)k * L.nall + r.c1];
+                if (rec == 1) {  // Darwish-Moukalled: R = x_c0 - x_c1 (psstValueReconstructor.cpp:105-107)
+                    r.o0[k] = (R)(x0 - x1);
+                } else if (rec == 2) {  // MUSCL: x_f - x_c per side
+                    r.o0[k] = (R)(xf - x0);
+                    r.o1[k] = (R)(xf - x1);
+                }
             }
+            out[d] = r;
         }
-        out[d] = r;
-    }
+    });
     (void)G;
     return out;
 }

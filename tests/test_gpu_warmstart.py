@@ -24,7 +24,7 @@ def test_learned_start_is_closer_and_converges_to_the_same_field():
     xs, ys = zip(*[ws.samples(c, g, s) for c, g, s in zip(TRAIN, grids, states)])
     X, Y = np.concatenate(xs), np.concatenate(ys)
     net = MLP(seed=3)
-    tr = ws.train(net, X, Y, epochs=600, batch=1024, lr=2e-3)
+    tr = ws.train(net, X, Y, epochs=600, batch=512, lr=2e-3)
     assert tr["loss"][-1] < 0.05 * tr["loss"][0]
 
     plain, tgrids, pstates = ws.solve_batch(TEST, 64, 3, 5, 12000, 200)
