@@ -238,7 +238,8 @@ psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *res_linf, do
 /* Reads of device arrays, reference volume order: "rho"[nvol] (density of
  * every volume, ghosts included, as psst_write_fluent needs it),
  * "residual"[(dim+2)*nvol], "dt"[nvol], "grad_u"[nvol*dim*dim],
- * "grad_p"[nvol*dim], "grad_T"[nvol*dim], "limiter"[nvol*(dim+2)]. */
+ * "grad_p"[nvol*dim], "grad_T"[nvol*dim] (with limiters 4/5 each gradient
+ * multiplied by its cell limiter psi, the form the MUSCL reconstruction uses). */
 psst_status psst_solver_get_array(psst_solver *s, const char *name, double *out, int64_t count);
 
 /* Runs the solver's work on the given CUDA stream (cudaStream_t passed as a

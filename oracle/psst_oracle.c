@@ -1201,13 +1201,14 @@ static void reconstruct(oracle_t *o, long f, prim_t r[2]) {
         pv[j][dim] = &r[j].p;
         pv[j][dim + 1] = &r[j].T;
     }
-    if (o->limiter >= 4) {
+    if (o->limiter >= 4) { /* phi_f = phi_c + (psi grad phi) . (x_f - x_c) */
         for (int j = 0; j < 2; ++j)
             for (int i = 0; i < dim + 2; ++i) {
                 const double *g = grad_of(o, vv[j], i);
+                const double psi = o->lim[vv[j] * NG + i];
                 double d = 0.0;
-                for (int k = 0; k < dim; ++k) d += g[k] * (o->xf[f * dim + k] - o->xc[vv[j] * dim + k]);
-                *pv[j][i] += o->lim[vv[j] * NG + i] * d;
+                for (int k = 0; k < dim; ++k) d += (g[k] * psi) * (o->xf[f * dim + k] - o->xc[vv[j] * dim + k]);
+                *pv[j][i] += d;
             }
     } else {
         double R[3];
@@ -1588,6 +1589,15 @@ long oracle_get(const oracle_t *o, const char *name, double *out, long cap) {
     if (!strcmp(name, "vol_grad_T")) COPY(nv * dim, o->g[((i / dim) * NG + dim + 1) * dim + i % dim]);
     if (!strcmp(name, "vol_grad_rho")) COPY(nv * dim, o->g[((i / dim) * NG + dim + 2) * dim + i % dim]);
     if (!strcmp(name, "vol_lim")) COPY(nv * (dim + 2), o->lim[(i / (dim + 2)) * NG + i % (dim + 2)]);
+    /* gradients as the reconstruction uses them: times psi with limiters 4/5 */
+    if (!strcmp(name, "vol_lgrad_u"))
+        COPY(nv * dim * dim, o->g[((i / (dim * dim)) * NG + (i % (dim * dim)) / dim) * dim + i % dim] *
+                                 (o->limiter >= 4 ? o->lim[(i / (dim * dim)) * NG + (i % (dim * dim)) / dim] : 1.0));
+    if (!strcmp(name, "vol_lgrad_p"))
+        COPY(nv * dim, o->g[((i / dim) * NG + dim) * dim + i % dim] * (o->limiter >= 4 ? o->lim[(i / dim) * NG + dim] : 1.0));
+    if (!strcmp(name, "vol_lgrad_T"))
+        COPY(nv * dim, o->g[((i / dim) * NG + dim + 1) * dim + i % dim] *
+                           (o->limiter >= 4 ? o->lim[(i / dim) * NG + dim + 1] : 1.0));
     if (!strcmp(name, "vol_zone")) COPY(nv, (double)o->vz[o->v_vz[i]].id);
     if (!strcmp(name, "vol_bc")) COPY(nv, (double)o->vz[o->v_vz[i]].bc);
     if (!strcmp(name, "vol_boundary")) COPY(nv, (double)o->v_boundary[i]);

@@ -16,11 +16,12 @@ struct alignas(16) CellRec {
 };
 enum { RP = 0, RT = 1, RRHO = 2, RU = 3 };
 
-// Gradients of u.., p, T (g[var * DIM + k]) and the cell limiter of each.
+// Gradients of u.., p, T (g[var * DIM + k]); with a cell limiter (MUSCL,
+// limiters 4/5) each variable's gradient is stored already multiplied by its
+// limiter psi. 64 bytes in 3D FP32 (15 values + padding).
 template <typename R, int DIM>
 struct alignas(16) GradRec {
     R g[(DIM + 2) * DIM];
-    R lim[DIM + 2];
 };
 
 // Face: neighbours (device ids), area, unit normal (FP64: geometry is kept in

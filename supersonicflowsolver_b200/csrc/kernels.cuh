@@ -193,8 +193,9 @@ __device__ __forceinline__ void boundary_flux(const Prim<R, DIM> &s, const R nn[
     flow[DIM + 1] = s.rho * vn * H;
 }
 
-// One side of the cell-limited MUSCL reconstruction: phi_f = phi_c + psi_c *
-// grad(phi)_c . (x_f - x_c); rho_f = p_f / (R T_f) as in the DM reconstruction.
+// One side of the cell-limited MUSCL reconstruction: phi_f = phi_c +
+// (psi_c grad(phi)_c) . (x_f - x_c), the record holding psi_c grad(phi)_c;
+// rho_f = p_f / (R T_f) as in the DM reconstruction.
 template <typename R, int DIM>
 __device__ __forceinline__ void muscl_side(Prim<R, DIM> &r, const GradRec<R, DIM> &gr, const R off[DIM], R rm) {
 #pragma unroll
@@ -202,7 +203,7 @@ __device__ __forceinline__ void muscl_side(Prim<R, DIM> &r, const GradRec<R, DIM
         R d = (R)0;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) d += gr.g[i * DIM + k] * off[k];
-        pvar<R, DIM>(r, i) += gr.lim[i] * d;
+        pvar<R, DIM>(r, i) += d;
     }
     r.rho = r.p / (rm * r.T);
 }
@@ -242,8 +243,7 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
         muscl_side<R, DIM>(r[1], *gr1, fr.o1, rm);
     }
     const R cp = (R)gas.cp, cv = (R)gas.cv, gamma = (R)gas.gamma;
-    R vn[2], a[2], H[2], M[2];
-    R fi[2][DIM + 2], wi[2][DIM + 2];
+    R vn[2], a[2], H[2], M[2], vsq[2];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         vn[j] = (R)0;
@@ -253,23 +253,25 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
             vn[j] += r[j].u[k] * nn[k];
             vs += r[j].u[k] * r[j].u[k];
         }
+        vsq[j] = vs;
         a[j] = sqrt(gamma * rm * r[j].T);
         H[j] = cp * r[j].T + (R)0.5 * vs;
-        if (FLUX == 1) {
-            M[j] = vn[j] / a[j];
-        } else {
-            const R E = cv * r[j].T + (R)0.5 * vs;
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) {
-                fi[j][k] = r[j].rho * r[j].u[k] * vn[j] + r[j].p * nn[k];
-                wi[j][k] = r[j].rho * r[j].u[k];
-            }
-            wi[j][DIM] = r[j].rho;
-            wi[j][DIM + 1] = r[j].rho * E;
-            fi[j][DIM] = r[j].rho * vn[j];
-            fi[j][DIM + 1] = r[j].rho * vn[j] * H[j];
-        }
+        if (FLUX == 1) M[j] = vn[j] / a[j];
     }
+    // physical flux f and conserved state w of side j, formed only in the
+    // branch that uses them (same expressions, so the same bits)
+    auto side = [&](int j, R f[DIM + 2], R w[DIM + 2]) {
+        const R E = cv * r[j].T + (R)0.5 * vsq[j];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            f[k] = r[j].rho * r[j].u[k] * vn[j] + r[j].p * nn[k];
+            w[k] = r[j].rho * r[j].u[k];
+        }
+        w[DIM] = r[j].rho;
+        w[DIM + 1] = r[j].rho * E;
+        f[DIM] = r[j].rho * vn[j];
+        f[DIM + 1] = r[j].rho * vn[j] * H[j];
+    };
     if (FLUX == 1) {  // psstConvectiveAUSM::calculate (psstConvectiveFlow.cpp:804-851)
         R Ms1, ps1, Ms0, ps0;
         if (M[1] >= (R)1) {
@@ -322,16 +324,21 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
     t = vRn + aR;
     if (s0 < t) s0 = t;
     if (FLUX == 2) {  // HLL (psstConvectiveFlow.cpp:268-286)
+        R f0[DIM + 2], w0[DIM + 2], f1[DIM + 2], w1[DIM + 2];
         if (s1 >= (R)0) {
+            side(1, f1, w1);
 #pragma unroll
-            for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[1][j];
+            for (int j = 0; j < DIM + 2; ++j) flow[j] = f1[j];
         } else if (s1 <= (R)0 && s0 >= (R)0) {
+            side(0, f0, w0);
+            side(1, f1, w1);
 #pragma unroll
             for (int j = 0; j < DIM + 2; ++j)
-                flow[j] = (s0 * fi[1][j] - s1 * fi[0][j] + s0 * s1 * (wi[0][j] - wi[1][j])) / (s0 - s1);
+                flow[j] = (s0 * f1[j] - s1 * f0[j] + s0 * s1 * (w0[j] - w1[j])) / (s0 - s1);
         } else if (s0 <= (R)0) {
+            side(0, f0, w0);
 #pragma unroll
-            for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[0][j];
+            for (int j = 0; j < DIM + 2; ++j) flow[j] = f0[j];
         } else {
             return false;
         }
@@ -341,17 +348,23 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
     const R p0 = r[0].p, p1 = r[1].p, d0 = r[0].rho, d1 = r[1].rho;
     const R sh = (p0 - p1 + d1 * vn[1] * (s1 - vn[1]) - d0 * vn[0] * (s0 - vn[0])) /
                  (d1 * (s1 - vn[1]) - d0 * (s0 - vn[0]));
+    R fs[DIM + 2], ws[DIM + 2];
     if (s1 >= (R)0) {
+        side(1, fs, ws);
 #pragma unroll
-        for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[1][j];
+        for (int j = 0; j < DIM + 2; ++j) flow[j] = fs[j];
     } else if ((s1 <= (R)0 && sh >= (R)0) || (sh <= (R)0 && s0 >= (R)0)) {
         const bool sd = (s1 <= (R)0 && sh >= (R)0);  // star state of side 1, else side 0
         const R ss = sd ? s1 : s0;
         const R tt = ss - sh;
         const R pr = sd ? r[1].p : r[0].p, dd = sd ? r[1].rho : r[0].rho, vv = sd ? vn[1] : vn[0];
+        if (sd)  // constant side indices: no dynamically indexed (local-memory) arrays
+            side(1, fs, ws);
+        else
+            side(0, fs, ws);
 #pragma unroll
         for (int j = 0; j < DIM + 2; ++j) {
-            const R wj = sd ? wi[1][j] : wi[0][j], fj = sd ? fi[1][j] : fi[0][j];
+            const R wj = ws[j], fj = fs[j];
             if (j < DIM)
                 flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * nn[j]) / tt;
             else if (j == DIM)
@@ -360,8 +373,9 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
                 flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * sh) / tt;
         }
     } else if (s0 <= (R)0) {
+        side(0, fs, ws);
 #pragma unroll
-        for (int j = 0; j < DIM + 2; ++j) flow[j] = fi[0][j];
+        for (int j = 0; j < DIM + 2; ++j) flow[j] = fs[j];
     } else {
         return false;
     }
@@ -477,8 +491,12 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
     R mx[NVAR], mn[NVAR];
 #pragma unroll
     for (int i = 0; i < NVAR; ++i) mx[i] = mn[i] = pvar<R, DIM>(own, i);
+    // FP64 (parity) path: the reference's arithmetic; FP32 path: one
+    // reciprocal of V per cell and fast divisions in the limiter
+    constexpr bool EXACT = sizeof(R) == 8;
     if (GRAD == 1) {
         const double V = g.V[c];
+        const double rV = EXACT ? 0.0 : 1.0 / V;
         for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
             const int32_t ent = g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
@@ -493,7 +511,7 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
                 }
             const R beta = (R)g.beta[f];
             const R rbeta = (R)1 - beta;
-            const R gp = (R)(fr.S / V);
+            const R gp = EXACT ? (R)(fr.S / V) : (R)(fr.S * rV);
             const R sgn = side ? (R)1 : (R)-1;
 #pragma unroll
             for (int i = 0; i < NVAR; ++i) {
@@ -549,13 +567,9 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
             }
         }
     }
-    GradRec<R, DIM> out;
+    R lim[NVAR];
 #pragma unroll
-    for (int i = 0; i < NVAR; ++i) {
-        out.lim[i] = (R)1;
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = gr[i][k];
-    }
+    for (int i = 0; i < NVAR; ++i) lim[i] = (R)1;
     if (CELLLIM) {
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
         for (int32_t q = 0; q < K; ++q) {
@@ -574,18 +588,23 @@ __global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, Dev
                 if (dm != (R)0) {
                     const R dp = dm > (R)0 ? mx[i] - phic : mn[i] - phic;
                     if (CELLLIM == 4) {
-                        const R y = dp / dm;
+                        const R y = EXACT ? dp / dm : (R)__fdividef((float)dp, (float)dm);
                         pf = y < (R)1 ? y : (R)1;
                     } else {
                         const R num = (dp * dp + eps2) + (R)2 * dm * dp;
                         const R den = dp * dp + (R)2 * dm * dm + dm * dp + eps2;
-                        pf = num / den;
+                        pf = EXACT ? num / den : (R)__fdividef((float)num, (float)den);
                     }
                 }
-                if (pf < out.lim[i]) out.lim[i] = pf;
+                if (pf < lim[i]) lim[i] = pf;
             }
         }
     }
+    GradRec<R, DIM> out;
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = CELLLIM ? gr[i][k] * lim[i] : gr[i][k];
     st16(reinterpret_cast<GradRec<R, DIM> *>(wk.grec) + c, out);
 }
 

@@ -793,7 +793,6 @@ void get_state(psst_solver *s, double *prim, double *wout) {
 
 template <typename R, int DIM>
 void grad_array(psst_solver *s, const std::string &nm, double *out) {
-    constexpr int NVAR = DIM + 2;
     const int32_t nint = s->L.nint;
     std::vector<GradRec<R, DIM>> h(nint);
     ck(cudaMemcpyAsync(h.data(), work<R>(s).grec, (size_t)nint * sizeof(GradRec<R, DIM>), cudaMemcpyDeviceToHost,
@@ -802,9 +801,7 @@ void grad_array(psst_solver *s, const std::string &nm, double *out) {
     ck(cudaStreamSynchronize(s->stream), "stream sync");
     for (int32_t d = 0; d < nint; ++d) {
         const int64_t v = s->L.vol_of_dev[d];
-        if (nm == "limiter") {
-            for (int i = 0; i < NVAR; ++i) out[v * NVAR + i] = (double)h[d].lim[i];
-        } else if (nm == "grad_u") {
+        if (nm == "grad_u") {
             for (int j = 0; j < DIM * DIM; ++j) out[v * DIM * DIM + j] = (double)h[d].g[j];
         } else {
             const int var = nm == "grad_p" ? DIM : DIM + 1;
@@ -851,9 +848,7 @@ void get_array(psst_solver *s, const std::string &nm, double *out, int64_t count
         return;
     }
     int64_t width;
-    if (nm == "limiter")
-        width = nvv;
-    else if (nm == "grad_u")
+    if (nm == "grad_u")
         width = (int64_t)dim * dim;
     else if (nm == "grad_p" || nm == "grad_T")
         width = dim;

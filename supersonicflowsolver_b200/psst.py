@@ -218,7 +218,7 @@ class Solver:
         check(_lib.load().psst_explicit_solve(self._h, int(n_iter), _ptr(linf), _ptr(l2)))
         return linf, l2
 
-    _ARR = {"rho": 1, "dt": 1, "residual": "nv", "limiter": "nv", "grad_u": "dd", "grad_p": "d", "grad_T": "d"}
+    _ARR = {"rho": 1, "dt": 1, "residual": "nv", "grad_u": "dd", "grad_p": "d", "grad_T": "d"}
 
     def get(self, name):
         w = self._ARR[name]

@@ -79,7 +79,7 @@ def test_fp64_bit_exact_per_iteration(tmp_path, tag, mesh, ckw, n, renumber):
         assert np.array_equal(s.get_state(), oracle_prim(o, nvol, dim)), "state, iteration %d" % (it + 1)
     assert np.array_equal(s.get("dt")[interior], o.get("vol_dt")[interior])
     if ckw.get("order", 2) == 2:
-        for k, ok in (("grad_p", "vol_grad_p"), ("grad_T", "vol_grad_T"), ("grad_u", "vol_grad_u")):
+        for k, ok in (("grad_p", "vol_lgrad_p"), ("grad_T", "vol_lgrad_T"), ("grad_u", "vol_lgrad_u")):
             w = s.get(k).reshape(nvol, -1)[interior]
             assert np.array_equal(w, o.get(ok).reshape(nvol, -1)[interior]), k
     _, w = s.get_state(with_w=True)
@@ -129,8 +129,8 @@ def test_fp64_cell_limiters_match_oracle(tmp_path, limiter, mesh):
     assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim))
     np.testing.assert_allclose(l2, ol2, rtol=1e-12, atol=0)
     interior = o.get("vol_bc") == 1
-    lim = s.get("limiter").reshape(g.nvol, -1)[interior]
-    assert np.array_equal(lim, o.get("vol_lim").reshape(g.nvol, -1)[interior])
+    for k in ("grad_p", "grad_T", "grad_u"):  # psi * gradient, as the reconstruction uses it
+        assert np.array_equal(s.get(k).reshape(g.nvol, -1)[interior], o.get("vol_l" + k).reshape(g.nvol, -1)[interior]), k
 
 
 @pytest.mark.parametrize("mesh", ["q", "t"])
