@@ -22,18 +22,21 @@
 
 #include "devgrid.hpp"
 
-// Register budgets of the three hot kernels (compile-time tuning; the values
-// are the measured best on the 6M-tet benchmark): k_face register cap,
-// k_cell and k_gradient minimum resident 256-thread blocks per SM.
+// Register budgets of the three hot kernels on the FP32 path (compile-time
+// tuning; the values are the measured best on the 6M-tet benchmark): k_face
+// register cap, k_cell and k_gradient minimum resident 256-thread blocks per
+// SM. The FP64 instantiations (twice the registers per value) get budgets
+// that do not spill.
 #ifndef PSST_FACE_MAXNREG
-#define PSST_FACE_MAXNREG 72
+#define PSST_FACE_MAXNREG 56
 #endif
 #ifndef PSST_CELL_MINB
 #define PSST_CELL_MINB 4
 #endif
 #ifndef PSST_GRAD_MINB
-#define PSST_GRAD_MINB 1
+#define PSST_GRAD_MINB 4
 #endif
+#define PSST_BUDGET(R, f32, f64) (sizeof(R) == 8 ? (f64) : (f32))
 
 namespace psst {
 
@@ -395,9 +398,9 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
 //   reference adds the two sound speeds in the opposite order on the other
 //   side; IEEE addition is commutative) and S;
 //  LocalAccTime2 (:189-193): S |n_k|.
-// Register cap PSST_FACE_MAXNREG (72: seven 128-thread blocks per SM, the tuned shape).
+// Register cap PSST_FACE_MAXNREG on the FP32 path (56: nine 128-thread blocks per SM).
 template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
-__global__ void __maxnreg__(PSST_FACE_MAXNREG) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
+__global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     using FO = FaceOut<R, DIM>;
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= g.nface) return;
@@ -472,7 +475,7 @@ __global__ void __maxnreg__(PSST_FACE_MAXNREG) k_face(DevGrid g, DevState<R> st,
 // Venkatakrishnan (AIAA 93-0880) cell limiter:
 // psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c).
 template <typename R, int DIM, int GRAD, int CELLLIM>
-__global__ void __launch_bounds__(256, PSST_GRAD_MINB) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
+__global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
     constexpr int NVAR = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nint) return;
@@ -882,7 +885,10 @@ template <int NV>
 __device__ __forceinline__ void last_block_finish(const double *part, unsigned *ticket,
                                                   int32_t nint, double *linf, double *l2, int it_slot) {
     __shared__ bool is_last;
-    __threadfence();
+    // the threads that wrote this block's partials (block_norm_partials) make
+    // them visible before the block takes its ticket; the other threads' own
+    // stores need no fence
+    if (threadIdx.x < NV) __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     __syncthreads();
@@ -942,7 +948,7 @@ __device__ __forceinline__ R lc1_normal_velocities(const FaceOut<R, DIM> &o, int
 }
 
 template <typename R, int DIM, int LC, bool BATCH>
-__global__ void __launch_bounds__(256, PSST_CELL_MINB) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
+__global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
                                               double cfl, double dt_uniform, double alpha, int stage,
                                               int it_slot) {
     // stage: bit 0 first stage of the iteration, bit 1 last stage
