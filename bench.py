@@ -151,8 +151,8 @@ def traffic_model(grid, nnz, kind):
     if kind == "face":
         # per face: face record read (64: c0,c1 (2i), S (g), n (3g), two FP32 offset vectors)
         # and the face output record written (32: flux*area 5s, time-step terms 3s);
-        # per interior cell: state record (32) + gradient/limiter record (80); ghosts: state (32)
-        return nf * (64 + 32) + nint * (32 + 80) + ngh * 32
+        # per interior cell: state record (32) + limited-gradient record (64); ghosts: state (32)
+        return nf * (64 + 32) + nint * (32 + 64) + ngh * 32
     if kind == "cell":
         # per cell: CSR ptr (i) + K entries (i) + K face areas (s) + own-order perm (8) + V (g) +
         # the stage-start FP64 state read (5x8) + new state record (32) + ghost ptr (i), and,
@@ -162,9 +162,9 @@ def traffic_model(grid, nnz, kind):
         S = SCHEME["rk_level"]
         return nint * (4 + 4 * K + 4 * K + 8 + 8 + 40 + 88.0 / S + 32 + 4) + nf * 32 + ngh * 72
     if kind == "gradient":
-        # per cell: CSR (i + K i) + perm + V + eps^2 + own state record (32) + gradient/limiter
-        # record written (80); per face: face record (64) + beta (g); ghosts: state record (32)
-        return nint * (4 + 4 * K + 8 + 8 + 8 + 32 + 80) + nf * 72 + ngh * 32
+        # per cell: CSR (i + K i) + perm + V + eps^2 + own state record (32) + limited-gradient
+        # record written (64); per face: face record (64) + beta (g); ghosts: state record (32)
+        return nint * (4 + 4 * K + 8 + 8 + 8 + 32 + 64) + nf * 72 + ngh * 32
     if kind == "ghost_update":
         return ngh * (12 + 20 + 20 + 24 + 24)
     return 0

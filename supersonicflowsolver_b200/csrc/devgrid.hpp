@@ -70,6 +70,7 @@ struct DevGrid {
     const double *V;          // [nint] cell volume
     const double *xc;         // [dim][nall] centroid (ghost: its face centre); least squares only
     const int32_t *csr_ptr;   // [nint+1]
+    int32_t kuni;             // K if every interior cell has K CSR entries (csr_ptr[c] = K c), else 0
     const int32_t *csr_ent;   // face << 1 | side, sorted by the reference's face-loop order
     const int32_t *csr_nb;    // the cell across each csr_ent face (saves a dependent load)
     const void *csr_s;        // R per csr_ent: the face's area, rounded to R (LocalAccTime1)

@@ -481,7 +481,9 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
     if (c >= g.nint) return;
     if (g.cell_case && !g.case_active[g.cell_case[c]]) return;  // stopped case
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
-    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    // uniform meshes (all tets, all hexes): the CSR range follows from c, one
+    // dependent load less
+    const int32_t b = g.kuni ? c * g.kuni : g.csr_ptr[c], K = g.kuni ? g.kuni : g.csr_ptr[c + 1] - b;
     const Prim<R, DIM> own = unpack<R, DIM>(ldg(st.rec + c));
     R gr[NVAR][DIM];
 #pragma unroll
@@ -969,7 +971,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
         const FO *fo = reinterpret_cast<const FO *>(wk.fout);
         const R *csr_s = reinterpret_cast<const R *>(g.csr_s);
         const RkIn<NV> rin = rk_load<R, NV>(g, wk, first_stage, c);
-        const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+        const int32_t b = g.kuni ? c * g.kuni : g.csr_ptr[c], K = g.kuni ? g.kuni : g.csr_ptr[c + 1] - b;
         const uint64_t perm = g.wperm[c];
         // When the cell's own face order is the face-loop order (the usual
         // case: faces are wired zone by zone in file order, and files list

@@ -939,6 +939,13 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
     g.nall = L.nall;
     g.nface = L.nface;
     g.nfi = L.nfi;
+    g.kuni = 0;
+    if (L.nint > 0) {
+        const int32_t k0 = L.csr_ptr[1] - L.csr_ptr[0];
+        bool uni = true;
+        for (int32_t d = 0; d < L.nint && uni; ++d) uni = L.csr_ptr[d + 1] - L.csr_ptr[d] == k0;
+        g.kuni = uni ? k0 : 0;
+    }
     g.beta = s->upload(L.beta);
     g.V = s->upload(L.V);
     g.xc = s->upload(L.xc);
