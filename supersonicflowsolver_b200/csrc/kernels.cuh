@@ -983,10 +983,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
         R den = (R)0, nnb = (R)0, s[DIM];
 #pragma unroll
         for (int k = 0; k < DIM; ++k) s[k] = (R)0;
-#pragma unroll 4
-        for (int32_t q = 0; q < K; ++q) {
-            const int32_t ent = g.csr_ent[b + q];
-            const FO o = ldg(fo + (ent >> 1));
+        // one CSR entry (face output o of entry ent, face area sa), in face-loop order
+        auto entry = [&](int32_t ent, const FO &o, R sa) {
             const int side = ent & 1;
             if (side) {
 #pragma unroll
@@ -999,11 +997,34 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
                 if (LC == 1) {
                     const R nv = lc1_normal_velocities<R, DIM>(o, side, nnb);
                     nnb = (nnb + nv) * (R)0.5;
-                    den += (fabs(nnb) + o.v[FO::CN]) * csr_s[b + q];
+                    den += (fabs(nnb) + o.v[FO::CN]) * sa;
                 } else if (LC == 2) {
 #pragma unroll
                     for (int k = 0; k < DIM; ++k) s[k] += o.v[FO::Q0 + k];
                 }
+            }
+        };
+        if (g.kuni == 4) {  // all-tet meshes: the four entries (b = 4c) as one 16-byte load each
+            const int4 e4 = *reinterpret_cast<const int4 *>(g.csr_ent + b);
+            R sa[4];
+            if constexpr (sizeof(R) == 4) {
+                const float4 t = *reinterpret_cast<const float4 *>(csr_s + b);
+                sa[0] = (R)t.x, sa[1] = (R)t.y, sa[2] = (R)t.z, sa[3] = (R)t.w;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sa[q] = csr_s[b + q];
+            }
+            const FO o0 = ldg(fo + (e4.x >> 1)), o1 = ldg(fo + (e4.y >> 1)), o2 = ldg(fo + (e4.z >> 1)),
+                     o3 = ldg(fo + (e4.w >> 1));
+            entry(e4.x, o0, sa[0]);
+            entry(e4.y, o1, sa[1]);
+            entry(e4.z, o2, sa[2]);
+            entry(e4.w, o3, sa[3]);
+        } else {
+#pragma unroll 4
+            for (int32_t q = 0; q < K; ++q) {
+                const int32_t ent = g.csr_ent[b + q];
+                entry(ent, ldg(fo + (ent >> 1)), csr_s[b + q]);
             }
         }
         double dt = dt_uniform;
