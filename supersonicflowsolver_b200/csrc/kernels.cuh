@@ -18,6 +18,7 @@
 // in-order gather of its faces' records, time step, RK update, its ghosts,
 // norms). Each interior face's flux is computed once.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 
 #include "devgrid.hpp"
@@ -79,6 +80,46 @@ __device__ __forceinline__ T ldg(const T *p) {
         for (int i = 0; i < (int)(sizeof(T) / 16); ++i) u.v[i] = q[i];
     }
     return u.t;
+}
+
+// The reconstruction offsets x_f - x_c of one side of a face record, reading
+// only the record's tail that holds them (the 32- or 16-byte chunks from the
+// one containing o0 to the end).
+template <typename R, int DIM>
+__device__ __forceinline__ void face_offsets(const FaceRec<R, DIM> *p, int side, R off[DIM]) {
+    using F = FaceRec<R, DIM>;
+    constexpr size_t CH = sizeof(F) % 32 == 0 ? 32 : 16;
+    constexpr size_t FROM = offsetof(F, o0) / CH * CH;
+    constexpr int NW = (int)((sizeof(F) - FROM) / 4);
+    union U {
+        uint32_t w[NW];
+        unsigned char b[NW * 4];
+        __device__ U() {}
+    } u;
+    const char *q = reinterpret_cast<const char *>(p) + FROM;
+    if constexpr (CH == 32) {
+#pragma unroll
+        for (int i = 0; i < NW / 8; ++i)
+            asm("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=r"(u.w[8 * i]), "=r"(u.w[8 * i + 1]), "=r"(u.w[8 * i + 2]), "=r"(u.w[8 * i + 3]),
+                  "=r"(u.w[8 * i + 4]), "=r"(u.w[8 * i + 5]), "=r"(u.w[8 * i + 6]), "=r"(u.w[8 * i + 7])
+                : "l"(q + 32 * i));
+    } else {
+#pragma unroll
+        for (int i = 0; i < NW / 4; ++i) {
+            const int4 v = *reinterpret_cast<const int4 *>(q + 16 * i);
+            u.w[4 * i] = (uint32_t)v.x, u.w[4 * i + 1] = (uint32_t)v.y, u.w[4 * i + 2] = (uint32_t)v.z,
+                   u.w[4 * i + 3] = (uint32_t)v.w;
+        }
+    }
+    constexpr size_t A0 = offsetof(F, o0) - FROM, A1 = offsetof(F, o1) - FROM;  // constant: stays in registers
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        R x0, x1;
+        memcpy(&x0, u.b + A0 + k * sizeof(R), sizeof(R));
+        memcpy(&x1, u.b + A1 + k * sizeof(R), sizeof(R));
+        off[k] = side ? x1 : x0;
+    }
 }
 
 // ld16: plain 128-bit loads, for records that other threads of the same
@@ -579,10 +620,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
         for (int32_t q = 0; q < K; ++q) {
             const int32_t ent = g.csr_ent[b + q];
-            const FaceRec<R, DIM> fr = ldg(frec + (ent >> 1));
             R off[DIM];  // x_f - x_c of this cell
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) off[k] = (ent & 1) ? fr.o1[k] : fr.o0[k];
+            face_offsets<R, DIM>(frec + (ent >> 1), ent & 1, off);
 #pragma unroll
             for (int i = 0; i < NVAR; ++i) {
                 const R phic = pvar<R, DIM>(own, i);

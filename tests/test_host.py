@@ -277,3 +277,24 @@ def test_adapted_case_file_round_trip(tmp_path):
         assert np.array_equal(g.get(k), g2.get(k)), k
     g2.write_fluent(prim, np.full(nv, 1.1766), str(tmp_path / "t2"))
     assert (tmp_path / "t2.cas").read_bytes() == (tmp_path / "t.cas").read_bytes()
+
+
+def test_host_geometry_independent_of_thread_count(tmp_path):
+    """Geometry and Green-Gauss weights are computed on all host threads; the
+    arrays are identical with one thread (a separate process, since the
+    thread count is read once)."""
+    import subprocess
+    import sys
+
+    m = meshgen.wedge3d(40, 20, 6, 12.0, tets=True)  # large enough to split into chunks
+    path, d, case = make_case(tmp_path, m)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); from supersonicflowsolver_b200.psst import Grid; "
+            "g = Grid.read_fluent(%r); np.savez(sys.argv[1], **{k: g.get(k) for k in %r})" % (ROOT, path, GEOM))
+    out = {}
+    for threads in ("1", "8"):
+        env = dict(os.environ, PSST_HOST_THREADS=threads)
+        f = str(tmp_path / ("geo%s.npz" % threads))
+        subprocess.run([sys.executable, "-c", code, f], check=True, env=env, timeout=300)
+        out[threads] = np.load(f)
+    for k in GEOM:
+        assert np.array_equal(out["1"][k], out["8"][k]), k
