@@ -50,12 +50,17 @@ CASES = [
     ("2d_adapted_hllc_vanleer", "a", dict(flux=3, order=2, limiter=3, lc=1), 4),
     ("2d_adapted_ausm_lsq_vanalbada_lc2", "a", dict(flux=1, order=2, limiter=1, lc=2, grad=2), 4),
     ("2d_adapted_hllc_bj", "a", dict(flux=3, order=2, limiter=4, lc=1), 4),
+    # smallest meshes: a block of one partly filled warp, cells with few interior neighbours
+    ("2d_two_cells_hllc_vanleer", "tiny2", dict(flux=3, order=2, limiter=3, lc=1), 4),
+    ("3d_six_tets_ausm_venkat_lc2", "tiny3", dict(flux=1, order=2, limiter=5, lc=2, mach=3.0), 3),
     # 3D least squares: corrected restatement (no reference counterpart)
     ("3d_tets_hllc_lsq_vanleer", "t", dict(flux=3, order=2, limiter=3, lc=1, grad=2, mach=3.0), 3),
     ("3d_hexes_ausm_lsq_venkat_lc2", "h", dict(flux=1, order=2, limiter=5, lc=2, grad=2, mach=3.0), 3),
 ]
 MESH = {
     "q": lambda: meshgen.wedge2d(30, 10, 15.0),
+    "tiny2": lambda: meshgen.wedge2d(2, 1, 15.0),  # two cells, every face but one on the boundary
+    "tiny3": lambda: meshgen.wedge3d(1, 1, 1, 12.0, tets=True),  # one hex split into six tets
     "j": lambda: meshgen.wedge2d(30, 10, 15.0, jitter=0.15, seed=3, shuffle_seed=1, interior_first=True),
     "t": lambda: meshgen.wedge3d(10, 5, 3, 12.0, tets=True),
     "h": lambda: meshgen.wedge3d(10, 5, 3, 12.0, tets=False, interior_first=True),
@@ -216,14 +221,17 @@ def test_deterministic(tmp_path):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("flux", [1, 2, 3], ids=["ausm", "hll", "hllc"])
-def test_fp32_close_to_fp64_oracle(tmp_path, flux):
+@pytest.mark.parametrize("flux,limiter,mesh", [(1, 3, "j"), (2, 3, "j"), (3, 3, "j"), (3, 5, "j"), (3, 4, "t")],
+                         ids=["ausm", "hll", "hllc", "hllc_venkat", "tets_hllc_bj"])
+def test_fp32_close_to_fp64_oracle(tmp_path, flux, limiter, mesh):
     """FP32 state/fluxes with FP64 geometry, RK state and norms: after 30
     iterations the primitive fields stay within 2e-4 relative of the FP64
     oracle (transient, before convergence; the converged error is reported by
-    the convergence study)."""
-    m = MESH["j"]()
-    path, d, name = make_case(tmp_path, m, max_iter=30, flux=flux, order=2, limiter=3, lc=1)
+    the convergence study). Cell limiters cover the FP32 MUSCL path (limited
+    gradient records, fast divisions in the limiter)."""
+    m = MESH[mesh]()
+    path, d, name = make_case(tmp_path, m, max_iter=30, flux=flux, order=2, limiter=limiter, lc=1,
+                              mach=3.0 if m.dim == 3 else 2.5)
     g, s = gpu_solver(path, d, name, precision=32, lc1_mode=1)
     o = Oracle(path, d, name, lc1_jacobi=1)
     s.explicit_solve(30)
