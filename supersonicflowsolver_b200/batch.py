@@ -88,6 +88,41 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None):
             "converged": int(sum(m.converged_at is not None for m in mons)), "cell_iterations": cells_run}
 
 
+def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chunk=100):
+    """FP32 until each case's residual has dropped by `switch` (above the FP32
+    floor, where FP32 still makes progress), then FP64 from the FP32 state
+    down to `drop`. Both phases judge the same absolute residual: the FP32
+    run's iterations 1..5 normalise it. Returns per-case FP32 and FP64
+    iterations, the wall time of the two phases and the hand-over (solver
+    set-up and launch-shape tuning excluded, as in run_batch), the final
+    state and the phases' cell-iterations."""
+    sc32 = type(scheme).from_buffer_copy(scheme)
+    sc32.precision = 32
+    sc64 = type(scheme).from_buffer_copy(scheme)
+    sc64.precision = 64
+    s32 = Solver(merged, sc32)
+    s64 = Solver(merged, sc64)
+    s32.set_state(merged.initial_state())
+    shapes = s32.autotune(2)
+    s32.use_graphs(True)
+    s64.launch_shape(shapes["gradient"], shapes["face"], shapes["cell"])
+    s64.use_graphs(True)
+    a = run_batch(s32, cells, drop=switch, max_iter=max_iter, chunk=chunk)
+    t0 = time.perf_counter()
+    s64.set_state(s32.get_state())
+    hand = time.perf_counter() - t0
+    s32.close()
+    b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"])
+    state = s64.get_state()
+    s64.close()
+    wall = a["wall_s"] + hand + b["wall_s"]
+    total = [None if (x is None or y is None) else x + y for x, y in zip(a["iterations"], b["iterations"])]
+    return {"iterations": total, "fp32_iterations": a["iterations"], "fp64_iterations": b["iterations"],
+            "switched": a["converged"], "converged": b["converged"], "wall_s": wall,
+            "fp32_wall_s": a["wall_s"], "fp64_wall_s": b["wall_s"], "handover_s": hand, "state": state,
+            "cell_iterations": a["cell_iterations"] + b["cell_iterations"], "threads_per_block": shapes}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--cases", type=int, default=256)
@@ -98,8 +133,32 @@ def main():
     ap.add_argument("--flux", type=int, default=3, help="1 AUSM, 2 HLL, 3 HLLC")
     ap.add_argument("--limiter", type=int, default=5)
     ap.add_argument("--precision", type=int, default=32)
+    ap.add_argument("--mixed", type=float, default=None, metavar="SWITCH",
+                    help="FP32 down to this residual drop, then FP64 to --drop")
     a = ap.parse_args()
     cases = sample_cases(a.cases, a.seed)
+    if a.mixed is not None:
+        with tempfile.TemporaryDirectory() as d:
+            t0 = time.perf_counter()
+            grids, sc = build_cases(cases, d, precision=32, flux=a.flux, limiter=a.limiter)
+            merged = Grid.merge(grids)
+            setup_s = time.perf_counter() - t0
+            r = run_mixed(merged, sc, [g.ninterior for g in grids], drop=a.drop, switch=a.mixed,
+                          max_iter=a.max_iter, chunk=a.chunk)
+        its = [x for x in r["iterations"] if x is not None]
+        f32 = [x for x in r["fp32_iterations"] if x is not None]
+        f64 = [x for x in r["fp64_iterations"] if x is not None]
+        print(json.dumps({"cases": a.cases, "seed": a.seed, "flux": a.flux, "limiter": a.limiter,
+                          "precision": "fp32 to %g, then fp64" % a.mixed, "cells": int(merged.ninterior),
+                          "setup_s": setup_s, "threads_per_block": r["threads_per_block"],
+                          "switched": r["switched"], "converged": r["converged"], "wall_s": r["wall_s"],
+                          "fp32_wall_s": r["fp32_wall_s"], "fp64_wall_s": r["fp64_wall_s"],
+                          "cell_updates_per_s": r["cell_iterations"] / r["wall_s"],
+                          "iterations_median": float(np.median(its)) if its else None,
+                          "iterations_max": max(its) if its else None,
+                          "fp32_iterations_median": float(np.median(f32)) if f32 else None,
+                          "fp64_iterations_median": float(np.median(f64)) if f64 else None}))
+        return
     with tempfile.TemporaryDirectory() as d:
         t0 = time.perf_counter()
         grids, sc = build_cases(cases, d, precision=a.precision, flux=a.flux, limiter=a.limiter)

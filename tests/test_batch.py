@@ -143,3 +143,26 @@ def test_merged_grid_limits(tmp_path):
     s = Solver(grids[0], schemes[0])
     with pytest.raises(PsstError):
         s.set_active([1])
+
+
+@pytest.mark.gpu
+def test_mixed_precision_batch_reaches_the_fp64_field(tmp_path):
+    """FP32 down to a 1e-4 drop, then FP64 from that state down to 1e-6:
+    every case converges and lands on the pure-FP64 converged field."""
+    from supersonicflowsolver_b200 import batch as bt
+    from supersonicflowsolver_b200.convergence import field_error
+
+    cases = [{"nx": 60, "ny": 20, "angle": a, "mach": m} for a, m in ((8.0, 2.5), (12.0, 3.1), (10.0, 2.2))]
+    grids, sc = bt.build_cases(cases, str(tmp_path), precision=32, flux=3, limiter=5)
+    merged = Grid.merge(grids)
+    cells = [g.ninterior for g in grids]
+    r = bt.run_mixed(merged, sc, cells, drop=1e-6, switch=1e-4, max_iter=20000, chunk=100)
+    assert r["switched"] == len(cases) and r["converged"] == len(cases)
+    sc64 = type(sc).from_buffer_copy(sc)
+    sc64.precision = 64
+    s = Solver(merged, sc64)
+    s.set_state(merged.initial_state())
+    p = bt.run_batch(s, cells, drop=1e-6, max_iter=20000, chunk=100)
+    assert p["converged"] == len(cases)
+    e = field_error(r["state"], s.get_state(), merged)
+    assert all(e[k]["rms_rel"] < 1e-5 for k in e), e
