@@ -56,15 +56,20 @@ def build_cases(cases, directory, precision=32, flux=3, limiter=5, cfl=0.5, rk_l
     return grids, scheme
 
 
-def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None):
+def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, caps=None):
     """Iterates all cases in chunks until every case reaches the residual drop
     (or max_iter); cells[i] = interior cells of case i; scales[i] (optional) a
-    fixed residual normalisation per case. Returns per-case iterations to the
-    drop, the normalisations used, timings and the cell-iterations of running
-    cases."""
+    fixed residual normalisation per case; caps[i] (optional) the iterations
+    case i may run here (it stops unconverged after them). Returns per-case
+    iterations to the drop, the normalisations used, timings and the
+    cell-iterations of running cases."""
     ncase = len(cells)
     mons = [DropMonitor(drop, scale=None if scales is None else scales[i]) for i in range(ncase)]
     active = np.ones(ncase, dtype=np.int32)
+    if caps is not None:
+        active[np.asarray(caps) <= 0] = 0
+        if not active.all():
+            solver.set_active(active)
     done, dev_s = 0, 0.0
     cells_run = 0
     t0 = time.perf_counter()
@@ -77,7 +82,7 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None):
         changed = False
         for i in np.flatnonzero(active):
             cells_run += int(cells[i]) * n
-            if mons[i].update(cols[:, i, :]):
+            if mons[i].update(cols[:, i, :]) or (caps is not None and done >= caps[i]):
                 active[i] = 0
                 changed = True
         if changed and active.any():
@@ -112,7 +117,9 @@ def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chu
     s64.set_state(s32.get_state())
     hand = time.perf_counter() - t0
     s32.close()
-    b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"])
+    # every case keeps the iteration budget of a pure run: max_iter in all
+    caps = [max_iter - (x if x is not None else a["run"]) for x in a["iterations"]]
+    b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"], caps=caps)
     state = s64.get_state()
     s64.close()
     wall = a["wall_s"] + hand + b["wall_s"]
