@@ -540,14 +540,24 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
     // FP64 (parity) path: the reference's arithmetic; FP32 path: one
     // reciprocal of V per cell and fast divisions in the limiter
     constexpr bool EXACT = sizeof(R) == 8;
+    // all-tet meshes: the four CSR entries and neighbours of the cell as two
+    // 16-byte loads up front (b = 4c), so each face costs one dependent load
+    // round trip instead of two
+    const bool u4 = g.kuni == 4;
+    int4 e4 = make_int4(0, 0, 0, 0), n4 = make_int4(0, 0, 0, 0);
+    if (u4) {
+        e4 = *reinterpret_cast<const int4 *>(g.csr_ent + b);
+        if (GRAD == 1) n4 = *reinterpret_cast<const int4 *>(g.csr_nb + b);
+    }
+    auto pick = [](const int4 &v, int32_t q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; };
     if (GRAD == 1) {
         const double V = g.V[c];
         const double rV = EXACT ? 0.0 : 1.0 / V;
         for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
-            const int32_t ent = g.csr_ent[b + q];
+            const int32_t ent = u4 ? pick(e4, q) : g.csr_ent[b + q];
             const int32_t f = ent >> 1, side = ent & 1;
             const FaceRec<R, DIM> fr = ldg(frec + f);
-            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + g.csr_nb[b + q]));
+            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + (u4 ? pick(n4, q) : g.csr_nb[b + q])));
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -619,7 +629,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
     if (CELLLIM) {
         const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
         for (int32_t q = 0; q < K; ++q) {
-            const int32_t ent = g.csr_ent[b + q];
+            const int32_t ent = u4 ? pick(e4, q) : g.csr_ent[b + q];
             R off[DIM];  // x_f - x_c of this cell
             face_offsets<R, DIM>(frec + (ent >> 1), ent & 1, off);
 #pragma unroll
