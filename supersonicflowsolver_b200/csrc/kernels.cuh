@@ -26,8 +26,9 @@
 // Register budgets of the three hot kernels on the FP32 path (compile-time
 // tuning; the values are the measured best on the 6M-tet benchmark): k_face
 // register cap, k_cell and k_gradient minimum resident 256-thread blocks per
-// SM. The FP64 instantiations (twice the registers per value) get budgets
-// that do not spill.
+// SM (gradient: 3, room for the pipelined loop's next-face records). The
+// FP64 instantiations (twice the registers per value) get budgets that do
+// not spill.
 #ifndef PSST_FACE_MAXNREG
 #define PSST_FACE_MAXNREG 56
 #endif
@@ -35,9 +36,12 @@
 #define PSST_CELL_MINB 4
 #endif
 #ifndef PSST_GRAD_MINB
-#define PSST_GRAD_MINB 4
+#define PSST_GRAD_MINB 3
 #endif
 #define PSST_BUDGET(R, f32, f64) (sizeof(R) == 8 ? (f64) : (f32))
+#ifndef PSST_GRAD_PIPE
+#define PSST_GRAD_PIPE 1  // software-pipelined Green-Gauss loop on all-tet meshes
+#endif
 
 namespace psst {
 
@@ -553,11 +557,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
     if (GRAD == 1) {
         const double V = g.V[c];
         const double rV = EXACT ? 0.0 : 1.0 / V;
-        for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
-            const int32_t ent = u4 ? pick(e4, q) : g.csr_ent[b + q];
-            const int32_t f = ent >> 1, side = ent & 1;
-            const FaceRec<R, DIM> fr = ldg(frec + f);
-            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + (u4 ? pick(n4, q) : g.csr_nb[b + q])));
+        auto face = [&](int32_t ent, const FaceRec<R, DIM> &fr, const Prim<R, DIM> &oth, R beta) {
+            const int32_t side = ent & 1;
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -565,7 +566,6 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
                     if (v > mx[i]) mx[i] = v;
                     if (v < mn[i]) mn[i] = v;
                 }
-            const R beta = (R)g.beta[f];
             const R rbeta = (R)1 - beta;
             const R gp = EXACT ? (R)(fr.S / V) : (R)(fr.S * rV);
             const R sgn = side ? (R)1 : (R)-1;
@@ -577,6 +577,32 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
 #pragma unroll
                 for (int k = 0; k < DIM; ++k) gr[i][k] += sgn * tv * gp * (R)fr.n[k];
             }
+        };
+#if PSST_GRAD_PIPE
+        if (u4) {  // software pipeline: the next face's records load while this face is summed
+            int32_t en = e4.x;
+            FaceRec<R, DIM> frn = ldg(frec + (en >> 1));
+            CellRec<R> recn = ldg(st.rec + n4.x);
+            R betan = (R)g.beta[en >> 1];
+            for (int32_t q = 0; q < 4; ++q) {
+                const int32_t ent = en;
+                const FaceRec<R, DIM> fr = frn;
+                const Prim<R, DIM> oth = unpack<R, DIM>(recn);
+                const R beta = betan;
+                if (q < 3) {
+                    en = pick(e4, q + 1);
+                    frn = ldg(frec + (en >> 1));
+                    recn = ldg(st.rec + pick(n4, q + 1));
+                    betan = (R)g.beta[en >> 1];
+                }
+                face(ent, fr, oth, beta);
+            }
+        } else
+#endif
+        for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
+            const int32_t ent = u4 ? pick(e4, q) : g.csr_ent[b + q];
+            face(ent, ldg(frec + (ent >> 1)), unpack<R, DIM>(ldg(st.rec + (u4 ? pick(n4, q) : g.csr_nb[b + q]))),
+                 (R)g.beta[ent >> 1]);
         }
     } else {
         constexpr int NR = DIM == 2 ? 3 : 7;  // r11 r12 r22 (r13 r23 r33 beta)
