@@ -30,7 +30,7 @@
 // FP64 instantiations (twice the registers per value) get budgets that do
 // not spill.
 #ifndef PSST_FACE_MAXNREG
-#define PSST_FACE_MAXNREG 56
+#define PSST_FACE_MAXNREG 48
 #endif
 #ifndef PSST_CELL_MINB
 #define PSST_CELL_MINB 4
@@ -443,7 +443,7 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
 //   reference adds the two sound speeds in the opposite order on the other
 //   side; IEEE addition is commutative) and S;
 //  LocalAccTime2 (:189-193): S |n_k|.
-// Register cap PSST_FACE_MAXNREG on the FP32 path (56: nine 128-thread blocks per SM).
+// Register cap PSST_FACE_MAXNREG on the FP32 path (48: ten 128-thread blocks per SM).
 template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
 __global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     using FO = FaceOut<R, DIM>;
