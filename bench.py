@@ -11,7 +11,8 @@ One step = one iteration (4 RK stages) over all cells. Synthetic mesh and
 freestream start: no dataset is involved.
 
   value : cell-updates/s with the state resident in HBM (K iterations in one
-          psst_explicit_solve call, CUDA events on the solver's stream)
+          psst_explicit_solve call, replayed as one CUDA graph captured
+          before the timed region; CUDA events on the solver's stream)
   e2e   : same metric through the C ABI with host buffers: the initial state
           copied from pinned host memory, K per-iteration psst_explicit_solve
           calls each returning its residual columns to the host, the final
@@ -330,7 +331,9 @@ def run_gpu(args):
     nint = grid.ninterior
     shapes = solver.autotune(3) if not args.no_autotune else solver.launch_shape()
     wl = WORKLOADS[args.workload]
-    if wl["dim"] == 2:  # a small mesh: launch latency dominates, replay whole calls as graphs
+    # replay whole explicit_solve calls as CUDA graphs (no launch gaps between
+    # the passes; on small meshes launch latency dominates)
+    if args.graphs == "on":
         solver.use_graphs(True)
 
     def barrier():
@@ -400,6 +403,7 @@ def run_gpu(args):
                                      if wl["precision"] == 32 else "FP64 throughout (the parity path)"),
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "threads_per_block": shapes,
+                       "cuda_graphs": args.graphs == "on",
                        "l2_flush": ("not needed: >2.5 GB of mesh + state per step, L2 is 126 MB" if wl["dim"] == 3
                                     else "none: this small case stays in L2 (not the bandwidth benchmark)")},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
@@ -438,6 +442,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wedge3d_6M_tets", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graphs", choices=["on", "off"], default="on",
+                    help="replay each explicit_solve call as a CUDA graph")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     args = ap.parse_args()
     if args.warmup < 3:
