@@ -400,6 +400,10 @@ struct psst_solver {
     int32_t *d_vol = nullptr;          // reference volume of each device cell
     double *d_prim = nullptr, *d_w = nullptr;  // reference-ordered state staging
     std::vector<int32_t> active_h;     // merged grids: per-case run flags (host copy)
+    // pinned host staging of a call's residual columns and error word: one
+    // stream synchronisation per call, no pageable-memory copies
+    double *hnorm = nullptr;
+    size_t hnorm_cap = 0;
     // CUDA graphs of whole psst_explicit_solve calls, keyed by (n_iter, buffer parity)
     bool use_graphs = false;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -430,6 +434,7 @@ struct psst_solver {
         if (device >= 0) cudaSetDevice(device);
         drop_graphs();
         for (void *p : allocs) cudaFree(p);
+        if (hnorm) cudaFreeHost(hnorm);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_stream) cudaStreamDestroy(own_stream);
@@ -529,12 +534,11 @@ void ensure_norms(psst_solver *s, int n_iter) {
     zero_norms<R>(s, n_iter);
 }
 
-void check_err(psst_solver *s, const int32_t *err_dev) {
-    int32_t e[4] = {0, 0, 0, 0};
-    ck(cudaMemcpyAsync(e, err_dev, sizeof e, cudaMemcpyDeviceToHost, s->stream), "err copy");
-    ck(cudaStreamSynchronize(s->stream), "stream sync");
+// e: the error word as copied to the host after the stream synchronised;
+// a set word is cleared on the device and raised.
+void raise_err(psst_solver *s, const int32_t e[4], const int32_t *err_dev) {
     if (e[0] == 0) return;
-    ck(cudaMemsetAsync((void *)err_dev, 0, sizeof e, s->stream), "memset");
+    ck(cudaMemsetAsync((void *)err_dev, 0, 4 * sizeof(int32_t), s->stream), "memset");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
     switch (e[0]) {
     case 1:
@@ -546,6 +550,13 @@ void check_err(psst_solver *s, const int32_t *err_dev) {
     default:
         raise(PSST_ERR_NONFINITE, "non-positive density or temperature in cell " + std::to_string(s->L.vol_of_dev[e[1]]));
     }
+}
+
+void check_err(psst_solver *s, const int32_t *err_dev) {
+    int32_t e[4] = {0, 0, 0, 0};
+    ck(cudaMemcpyAsync(e, err_dev, sizeof e, cudaMemcpyDeviceToHost, s->stream), "err copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    raise_err(s, e, err_dev);
 }
 
 enum Kind { K_GRADIENT = 0, K_FACE = 1, K_CELL = 2, K_GHOST = 3, K_NORM = 4 };
@@ -634,18 +645,33 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     }
     ck(cudaEventRecord(s->ev1, s->stream), "event");
     ck(cudaGetLastError(), "kernel launch");
-    std::vector<double> li((size_t)n_iter * s->nv), l2((size_t)n_iter * s->nv);
-    ck(cudaMemcpyAsync(li.data(), w.linf, li.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
-    ck(cudaMemcpyAsync(l2.data(), w.l2, l2.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
-    check_err(s, w.err);
+    // residual columns and the error word into pinned staging, one sync
+    const size_t nn = (size_t)n_iter * s->nv, need = 2 * nn + 2;
+    if (s->hnorm_cap < need) {
+        if (s->hnorm) cudaFreeHost(s->hnorm);
+        s->hnorm = nullptr;
+        s->hnorm_cap = 0;
+        ck(cudaMallocHost(reinterpret_cast<void **>(&s->hnorm), need * sizeof(double)), "cudaMallocHost");
+        s->hnorm_cap = need;
+    }
+    double *li = s->hnorm, *l2 = s->hnorm + nn;
+    int32_t *he = reinterpret_cast<int32_t *>(s->hnorm + 2 * nn);
+    ck(cudaMemcpyAsync(li, w.linf, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
+    ck(cudaMemcpyAsync(l2, w.l2, nn * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
+    ck(cudaMemcpyAsync(he, w.err, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream), "err copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    {
+        const int32_t e[4] = {he[0], he[1], he[2], he[3]};
+        raise_err(s, e, w.err);
+    }
     float ms = 0.0f;
     ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
     s->last_ms = ms;
     s->last_launches = launches;
     s->last_n = n_iter;
     s->iter += n_iter;
-    if (res_linf) std::memcpy(res_linf, li.data(), li.size() * sizeof(double));
-    if (res_l2) std::memcpy(res_l2, l2.data(), l2.size() * sizeof(double));
+    if (res_linf) std::memcpy(res_linf, li, nn * sizeof(double));
+    if (res_l2) std::memcpy(res_l2, l2, nn * sizeof(double));
 }
 
 template <typename R>
