@@ -317,7 +317,6 @@ psst_status psst_convective_residual_static(int32_t dim, int32_t flux, int32_t n
                                             const double *prim, double rm, double cp, double cv, double gamma,
                                             double *residual, void *stream);
 
-/* Reference counter psstGridFV::iter_ after the calls so far. */
 /* No counterpart in the reference. With on != 0, each psst_explicit_solve
  * call is captured once as a CUDA graph (per iteration count and state-buffer
  * parity) and replayed afterwards: one launch per call instead of one per
@@ -335,6 +334,29 @@ psst_status psst_solver_set_active(psst_solver *s, const int32_t *active);
  * cells of |res| (the reference's column, per case). n_iter <= that call's. */
 psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, double *out);
 
+/* Sequential LocalAccTime1 (lc1_mode SEQUENTIAL, FP64, single grids): the
+ * reference's in-loop order (psstFiniteVolumeGrid.cpp:317-323) as a wavefront.
+ * With on != 0 (the default) each psst_explicit_solve call runs as ONE
+ * persistent cooperative launch: operation m (a gradient or an RK stage) of a
+ * cell at level L runs at step P m + L, so the operations of many iterations
+ * overlap along the level chain, every cell keeps the reference's inputs and
+ * results are bit-identical to the level-by-level walk (on == 0, one launch
+ * sequence per stage, also the path of the stage-by-stage API). Calls are not
+ * captured as CUDA graphs in this mode. */
+psst_status psst_solver_use_wavefront(psst_solver *s, int on);
+
+/* Bound of each device-side wait of the persistent launch (its grid
+ * barriers), in nanoseconds; < 0 restores the default (10 s). A wait that runs
+ * out stops the launch and the call returns PSST_ERR_TIMEOUT; the solver stays
+ * usable, its state is undefined until the next psst_solver_set_state. 0 makes
+ * every wait run out at once (used to test that path). */
+psst_status psst_solver_set_wait_limit(psst_solver *s, int64_t nanoseconds);
+
+/* Schedule of the sequential LocalAccTime1: info[5] = {wavefront active (0/1),
+ * period P, levels, work items, CTAs of the persistent launch}. */
+psst_status psst_solver_schedule_info(const psst_solver *s, int64_t *info);
+
+/* Reference counter psstGridFV::iter_ after the calls so far. */
 int64_t psst_solver_iter(const psst_solver *s);
 
 void psst_solver_destroy(psst_solver *s);

@@ -124,4 +124,47 @@ struct Gas {
     double rm, cp, cv, gamma;
 };
 
+// Wavefront schedule of the sequential LocalAccTime1 (the reference's in-loop
+// order, psstFiniteVolumeGrid.cpp:317-323) over many RK stages in one
+// persistent launch. Cell c's level exceeds the level of every interior
+// neighbour updated before it; D is the largest level difference across an
+// interior face and P = D + 1. Operation m of the call (a gradient or an RK
+// stage) of cell c runs at step P m + level(c): every input it needs -- the
+// previous operation of each neighbour and this operation of each earlier
+// neighbour -- is then at least one step (one grid barrier) old. Work items
+// are chunks (at most one block) of one level; they are ordered by level mod
+// P, then level, so the items of one step are contiguous.
+struct WfSched {
+    int32_t period;          // P
+    int32_t nlevels, nitems;
+    const int32_t *cells;       // [nint] interior cells in item order
+    const int32_t *item_ptr;    // [nitems+1] cell range of each item in `cells`
+    const int32_t *item_level;  // [nitems]
+    const int32_t *lvl_items;   // [2 nlevels] item range [first, end) of each level
+    double *ipart;              // [2][nitems][2 NV] per item: sum res^2, max |res| (by operation parity)
+    double *acc;                // [nacc][2 NV] per RK stage: the same over the levels folded so far
+    int32_t nacc;
+    void *grec2;                // second gradient buffer (gradients by iteration parity)
+    unsigned *sync;             // [4] grid barrier: arrivals, generation, abort flag
+};
+
+template <typename R>
+struct WfArgs {
+    DevGrid g;
+    CellRec<R> *buf[2];  // state buffers; a stage reads one and writes the other
+    DevWork<R> wk;
+    void *gbuf[2];       // gradient buffers of the iterations n-1, n-3, .. ([0]) and n-2, .. ([1])
+    WfSched sc;
+    Gas gas;
+    double cfl;
+    double alpha[16];
+    int32_t nst;      // RK stages per iteration
+    int32_t nopi;     // operations per iteration: nst, + 1 with a gradient
+    int64_t nops;     // operations of the call
+    int32_t n_iter;
+    int32_t flux, grad, celllim;
+    int32_t in_buf;   // buffer holding the call's input state
+    uint64_t wait_ns; // bound of each grid-barrier wait (0: do not wait)
+};
+
 }  // namespace psst

@@ -45,7 +45,7 @@
 
 namespace psst {
 
-enum ErrCode { ERR_HLL = 1, ERR_HLLC = 2, ERR_NONFINITE_RES = 3, ERR_BAD_STATE = 4 };
+enum ErrCode { ERR_HLL = 1, ERR_HLLC = 2, ERR_NONFINITE_RES = 3, ERR_BAD_STATE = 4, ERR_TIMEOUT = 5 };
 
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -141,6 +141,40 @@ __device__ __forceinline__ T ld16(const T *p) {
     for (int i = 0; i < (int)(sizeof(T) / 16); ++i) u.v[i] = q[i];
     return u.t;
 }
+// ldcg: 128-bit loads through L2 only (ld.global.cg), for records that other
+// CTAs of a persistent launch write between its grid barriers: an L1-cached
+// load could return a line this SM kept from before the write. Volatile, so
+// the compiler neither merges nor hoists it across steps.
+template <typename T>
+__device__ __forceinline__ T ldcg(const T *p) {
+    static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
+    union U {
+        T t;
+        uint32_t w[sizeof(T) / 4];
+        __device__ U() {}
+    } u;
+    const char *q = reinterpret_cast<const char *>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(T) / 16); ++i)
+        asm volatile("ld.global.cg.v4.b32 {%0,%1,%2,%3}, [%4];"
+                     : "=r"(u.w[4 * i]), "=r"(u.w[4 * i + 1]), "=r"(u.w[4 * i + 2]), "=r"(u.w[4 * i + 3])
+                     : "l"(q + 16 * i));
+    return u.t;
+}
+__device__ __forceinline__ double ldcg(const double *p) {
+    double v;
+    asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+// state and gradient records: ldg in the pass kernels, ldcg in the persistent one
+template <bool CG, typename T>
+__device__ __forceinline__ T ldst(const T *p) {
+    if constexpr (CG)
+        return ldcg(p);
+    else
+        return ldg(p);
+}
+
 template <typename T>
 __device__ __forceinline__ void st16(T *p, const T &t) {
     static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
@@ -519,17 +553,18 @@ __global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGr
 // (Anderson & Bonhaus 1994), then the reference's theta corrections. Then, for limiters 4/5, the Barth-Jespersen (AIAA 89-0366) /
 // Venkatakrishnan (AIAA 93-0880) cell limiter:
 // psi = min over faces of phi(Delta+, Delta-), Delta- = grad . (x_f - x_c).
-template <typename R, int DIM, int GRAD, int CELLLIM>
-__global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
+// Gradient (and cell limiter) of one interior cell c from the state records
+// `rec`, written to out[c]. CG: state loads through L2 only (the persistent
+// wavefront kernel, where other CTAs write the states between its steps).
+template <typename R, int DIM, int GRAD, int CELLLIM, bool CG>
+__device__ __forceinline__ void gradient_cell(const DevGrid &g, const CellRec<R> *rec, GradRec<R, DIM> *gout,
+                                              int32_t c) {
     constexpr int NVAR = DIM + 2;
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.nint) return;
-    if (g.cell_case && !g.case_active[g.cell_case[c]]) return;  // stopped case
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     // uniform meshes (all tets, all hexes): the CSR range follows from c, one
     // dependent load less
     const int32_t b = g.kuni ? c * g.kuni : g.csr_ptr[c], K = g.kuni ? g.kuni : g.csr_ptr[c + 1] - b;
-    const Prim<R, DIM> own = unpack<R, DIM>(ldg(st.rec + c));
+    const Prim<R, DIM> own = unpack<R, DIM>(ldst<CG>(rec + c));
     R gr[NVAR][DIM];
 #pragma unroll
     for (int i = 0; i < NVAR; ++i)
@@ -582,7 +617,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
         if (u4) {  // software pipeline: the next face's records load while this face is summed
             int32_t en = e4.x;
             FaceRec<R, DIM> frn = ldg(frec + (en >> 1));
-            CellRec<R> recn = ldg(st.rec + n4.x);
+            CellRec<R> recn = ldst<CG>(rec + n4.x);
             R betan = (R)g.beta[en >> 1];
             for (int32_t q = 0; q < 4; ++q) {
                 const int32_t ent = en;
@@ -592,7 +627,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
                 if (q < 3) {
                     en = pick(e4, q + 1);
                     frn = ldg(frec + (en >> 1));
-                    recn = ldg(st.rec + pick(n4, q + 1));
+                    recn = ldst<CG>(rec + pick(n4, q + 1));
                     betan = (R)g.beta[en >> 1];
                 }
                 face(ent, fr, oth, beta);
@@ -601,7 +636,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
 #endif
         for (int32_t q = 0; q < K; ++q) {  // not unrolled: fewer registers, more blocks (measured faster)
             const int32_t ent = u4 ? pick(e4, q) : g.csr_ent[b + q];
-            face(ent, ldg(frec + (ent >> 1)), unpack<R, DIM>(ldg(st.rec + (u4 ? pick(n4, q) : g.csr_nb[b + q]))),
+            face(ent, ldg(frec + (ent >> 1)), unpack<R, DIM>(ldst<CG>(rec + (u4 ? pick(n4, q) : g.csr_nb[b + q]))),
                  (R)g.beta[ent >> 1]);
         }
     } else {
@@ -614,7 +649,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
         for (int32_t j = 0; j < K; ++j) {
             const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
             const int32_t nb = g.csr_nb[slot];
-            const Prim<R, DIM> oth = unpack<R, DIM>(ldg(st.rec + nb));
+            const Prim<R, DIM> oth = unpack<R, DIM>(ldst<CG>(rec + nb));
             if (CELLLIM)
 #pragma unroll
                 for (int i = 0; i < NVAR; ++i) {
@@ -685,7 +720,15 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
     for (int i = 0; i < NVAR; ++i)
 #pragma unroll
         for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = CELLLIM ? gr[i][k] * lim[i] : gr[i][k];
-    st16(reinterpret_cast<GradRec<R, DIM> *>(wk.grec) + c, out);
+    st16(gout + c, out);
+}
+
+template <typename R, int DIM, int GRAD, int CELLLIM>
+__global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_gradient(DevGrid g, DevState<R> st, DevWork<R> wk) {
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.nint) return;
+    if (g.cell_case && !g.case_active[g.cell_case[c]]) return;  // stopped case
+    gradient_cell<R, DIM, GRAD, CELLLIM, false>(g, st.rec, reinterpret_cast<GradRec<R, DIM> *>(wk.grec), c);
 }
 
 // cell update
@@ -693,8 +736,9 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_GRAD_MINB, 1)) k_grad
 
 // Local time step of one cell (psstLocalTimeCalculation.cpp:90-131, 175-213),
 // faces in the cell's own order. In the sequential mode, neighbours updated
-// earlier in the reference's order are read from `nxt`.
-template <typename R, int DIM, int LC, bool SEQ>
+// earlier in the reference's order are read from `nxt`. CG: neighbour states
+// through L2 only (the persistent wavefront kernel).
+template <typename R, int DIM, int LC, bool SEQ, bool CG = false>
 __device__ __forceinline__ double local_time(const DevGrid &g, const CellRec<R> *cur, const CellRec<R> *nxt,
                                              const Gas &gas, double cfl, double dt_uniform, int32_t c,
                                              const Prim<R, DIM> &own) {
@@ -714,7 +758,7 @@ __device__ __forceinline__ double local_time(const DevGrid &g, const CellRec<R> 
             const FaceRec<R, DIM> fr = ld16(frec + (ent >> 1));
             const int32_t nb = (ent & 1) ? fr.c0 : fr.c1;
             const CellRec<R> *src = (SEQ && nb < g.nint && g.rank[nb] < myrank) ? nxt : cur;
-            const Prim<R, DIM> o = unpack<R, DIM>(ld16(src + nb));
+            const Prim<R, DIM> o = unpack<R, DIM>(CG ? ldcg(src + nb) : ld16(src + nb));
             const R cn = (sqrt(gr * o.T) + cc) * (R)0.5;
             R nv = (R)0;
 #pragma unroll

@@ -11,6 +11,7 @@ namespace psst {
 
 constexpr int kBlock = 256;
 constexpr int kMinBlock = 64;  // smallest launch shape the tuner may pick
+constexpr int kWfBlock = 128;  // threads per CTA of k_wavefront (and cells per work item)
 inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
 template <typename R>
@@ -51,6 +52,11 @@ struct Ops {
     static void ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                              const Gas &gas, cudaStream_t s);
     static void norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s);
+    // Sequential LocalAccTime1 over a whole call as one cooperative launch of
+    // nblocks CTAs (k_wavefront; FP64 only, cudaErrorNotSupported otherwise).
+    static cudaError_t wavefront(int dim, int rec, int lim, const WfArgs<R> &a, int nblocks, cudaStream_t s);
+    // co-resident CTAs of that kernel on the current device (0: not built)
+    static int wavefront_max_blocks(int dim, int rec, int lim);
 };
 
 }  // namespace psst

@@ -3,6 +3,7 @@
 #pragma once
 #include "kernels.cuh"
 #include "ops.hpp"
+#include "wavefront.cuh"
 
 namespace psst {
 
@@ -232,6 +233,44 @@ void Ops<R>::norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, 
         k_norm_finish<4><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
     else
         k_norm_finish<5><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
+}
+
+// ---- sequential LocalAccTime1 as one persistent launch (FP64 only) ----
+template <typename R, int DIM>
+static cudaError_t wavefront_d(int rec, int lim, const WfArgs<R> &a, int nb, cudaStream_t s) {
+    if (rec == 0) return wf_launch<R, DIM, 0, 1>(a, nb, s);
+    if (rec == 2) return wf_launch<R, DIM, 2, 1>(a, nb, s);
+    if (lim == 1) return wf_launch<R, DIM, 1, 1>(a, nb, s);
+    if (lim == 2) return wf_launch<R, DIM, 1, 2>(a, nb, s);
+    return wf_launch<R, DIM, 1, 3>(a, nb, s);
+}
+template <typename R, int DIM>
+static int wavefront_max_d(int rec, int lim) {
+    if (rec == 0) return wf_max_blocks<R, DIM, 0, 1>();
+    if (rec == 2) return wf_max_blocks<R, DIM, 2, 1>();
+    if (lim == 1) return wf_max_blocks<R, DIM, 1, 1>();
+    if (lim == 2) return wf_max_blocks<R, DIM, 1, 2>();
+    return wf_max_blocks<R, DIM, 1, 3>();
+}
+
+template <typename R>
+cudaError_t Ops<R>::wavefront(int dim, int rec, int lim, const WfArgs<R> &a, int nb, cudaStream_t s) {
+    if constexpr (sizeof(R) == 8) {
+        return dim == 2 ? wavefront_d<R, 2>(rec, lim, a, nb, s) : wavefront_d<R, 3>(rec, lim, a, nb, s);
+    } else {
+        (void)dim, (void)rec, (void)lim, (void)a, (void)nb, (void)s;
+        return cudaErrorNotSupported;
+    }
+}
+
+template <typename R>
+int Ops<R>::wavefront_max_blocks(int dim, int rec, int lim) {
+    if constexpr (sizeof(R) == 8) {
+        return dim == 2 ? wavefront_max_d<R, 2>(rec, lim) : wavefront_max_d<R, 3>(rec, lim);
+    } else {
+        (void)dim, (void)rec, (void)lim;
+        return 0;
+    }
 }
 
 }  // namespace psst

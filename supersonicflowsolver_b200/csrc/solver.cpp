@@ -74,6 +74,9 @@ struct Layout {
     std::vector<int32_t> dev_of_vol;  // reference volume -> device cell (-1: inactive)
     std::vector<int64_t> vol_of_dev;  // device cell -> reference volume
     std::vector<int32_t> c0, c1, csr_ptr, csr_ent, csr_nb, rank, gptr, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
+    // wavefront schedule of the sequential LocalAccTime1 (WfSched)
+    int32_t wf_period = 1, wf_max_class_items = 0;
+    std::vector<int32_t> wf_cells, wf_item_ptr, wf_item_level, wf_lvl_items;
     std::vector<uint64_t> wperm;
     std::vector<double> S, n, xf, beta, V, xc, lsq_r, vk_eps2, z_u, z_p, z_T;
 };
@@ -337,6 +340,39 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         const int32_t d = dev_by_rank[r];
         L.lvl_cells[fillp[level[d]]++] = d;
     }
+    // wavefront schedule: period P = 1 + the largest level difference across
+    // an interior face; items of at most kWfBlock cells of one level (device
+    // order inside a level), ordered by level mod P, then level
+    if (sc.lc == 1 && sc.lc1_mode == PSST_LC1_SEQUENTIAL && L.nint > 0) {
+        int32_t D = 0;
+        for (int32_t d = 0; d < L.nint; ++d)
+            for (int32_t q = L.csr_ptr[d]; q < L.csr_ptr[d + 1]; ++q) {
+                const int32_t nb = L.csr_nb[q];
+                if (nb < L.nint) D = std::max(D, std::abs(level[d] - level[nb]));
+            }
+        L.wf_period = D + 1;
+        std::vector<int32_t> by_level(L.nint), fill(L.lvl_ptr.begin(), L.lvl_ptr.end() - 1);
+        for (int32_t d = 0; d < L.nint; ++d) by_level[fill[level[d]]++] = d;
+        L.wf_lvl_items.assign((size_t)2 * L.nlevels, 0);
+        L.wf_cells.clear();
+        L.wf_item_ptr.clear();
+        L.wf_item_level.clear();
+        for (int32_t r = 0; r < L.wf_period; ++r) {
+            const int32_t first = (int32_t)L.wf_item_level.size();
+            for (int32_t l = r; l < L.nlevels; l += L.wf_period) {
+                L.wf_lvl_items[2 * (size_t)l] = (int32_t)L.wf_item_level.size();
+                for (int32_t b = L.lvl_ptr[l]; b < L.lvl_ptr[l + 1]; b += kWfBlock) {
+                    L.wf_item_ptr.push_back((int32_t)L.wf_cells.size());
+                    L.wf_item_level.push_back(l);
+                    for (int32_t i = b; i < std::min(b + kWfBlock, L.lvl_ptr[l + 1]); ++i)
+                        L.wf_cells.push_back(by_level[i]);
+                }
+                L.wf_lvl_items[2 * (size_t)l + 1] = (int32_t)L.wf_item_level.size();
+            }
+            L.wf_max_class_items = std::max(L.wf_max_class_items, (int32_t)L.wf_item_level.size() - first);
+        }
+        L.wf_item_ptr.push_back((int32_t)L.wf_cells.size());
+    }
 }
 
 
@@ -408,6 +444,14 @@ struct psst_solver {
     bool use_graphs = false;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, int>, int64_t> graph_launches;
+    // sequential LocalAccTime1 as one persistent launch per call (FP64, single
+    // grids): schedule uploaded (wf_ready), switched on (wf_on), CTAs, and the
+    // bound of every grid-barrier wait
+    bool wf_ready = false, wf_on = true;
+    WfSched wf{};
+    int wf_blocks = 0;
+    uint64_t wait_ns = kDefaultWaitNs;
+    static constexpr uint64_t kDefaultWaitNs = 10000000000ull;  // 10 s; a step takes microseconds
 
     void drop_graphs() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -547,6 +591,9 @@ void raise_err(psst_solver *s, const int32_t e[4], const int32_t *err_dev) {
         raise(PSST_ERR_FLUX, "Error: Could not calculate convective HLLC flow!");
     case 3:
         raise(PSST_ERR_NONFINITE, "non-finite residual in cell " + std::to_string(s->L.vol_of_dev[e[1]]));
+    case 5:
+        raise(PSST_ERR_TIMEOUT, "a grid-barrier wait of the wavefront launch ran out (step " + std::to_string(e[1]) +
+                                    "); the state is undefined until the next psst_solver_set_state");
     default:
         raise(PSST_ERR_NONFINITE, "non-positive density or temperature in cell " + std::to_string(s->L.vol_of_dev[e[1]]));
     }
@@ -593,9 +640,47 @@ void one_stage(psst_solver *s, int k, int it_slot, bool gather, Mark &&mark) {
     s->cur ^= 1;
 }
 
+bool wavefront_active(const psst_solver *s) { return s->seq && s->wf_ready && s->wf_on; }
+
+// The whole call as one cooperative launch (the wavefront schedule, WfSched);
+// the norm buffers are reserved and zeroed by the caller.
+template <typename R>
+void wavefront_run(psst_solver *s, int n_iter) {
+    DevState<R> *st = states<R>(s);
+    DevWork<R> &w = work<R>(s);
+    ck(cudaMemsetAsync(s->wf.sync, 0, 4 * sizeof(unsigned), s->stream), "memset");
+    WfArgs<R> a{};
+    a.g = s->g;
+    a.buf[0] = st[0].rec;
+    a.buf[1] = st[1].rec;
+    a.wk = w;
+    a.gbuf[0] = w.grec;
+    a.gbuf[1] = s->wf.grec2;
+    a.sc = s->wf;
+    a.gas = s->gas;
+    a.cfl = s->sc.cfl;
+    for (int k = 0; k < 16; ++k) a.alpha[k] = s->sc.rk[k];
+    a.nst = s->sc.rk_level;
+    a.nopi = a.nst + (s->sc.order == 2 ? 1 : 0);
+    a.nops = (int64_t)n_iter * a.nopi;
+    a.n_iter = n_iter;
+    a.flux = s->sc.flux;
+    a.grad = s->sc.grad;
+    a.celllim = s->celllim;
+    a.in_buf = s->cur;
+    a.wait_ns = s->wait_ns;
+    ck(Ops<R>::wavefront(s->dim, s->rec, s->sc.limiter, a, s->wf_blocks, s->stream), "wavefront launch");
+    s->cur = (int)((s->cur + (int64_t)n_iter * a.nst) & 1);
+}
+
 template <typename R, typename Mark>
 void iterations(psst_solver *s, int n_iter, Mark &&mark) {
     DevWork<R> &w = work<R>(s);
+    if (wavefront_active(s)) {
+        wavefront_run<R>(s, n_iter);
+        mark(K_CELL);
+        return;
+    }
     for (int it = 0; it < n_iter; ++it) {
         if (s->sc.order == 2) {
             Ops<R>::gradient(s->dim, s->sc.grad, s->celllim, s->g, states<R>(s)[s->cur], w, s->stream);
@@ -613,7 +698,7 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     reserve_norms<R>(s, n_iter);
     int64_t launches = 0;
     ck(cudaEventRecord(s->ev0, s->stream), "event");
-    if (s->use_graphs) {
+    if (s->use_graphs && !wavefront_active(s)) {  // a wavefront call is one launch already
         const std::pair<int, int> key(n_iter, s->cur);
         auto it = s->graphs.find(key);
         if (it == s->graphs.end()) {
@@ -1010,6 +1095,27 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
         alloc_state<float>(s.get(), *G);
     else
         alloc_state<double>(s.get(), *G);
+    if (s->seq && sc->precision == 64 && L.cell_case.empty() && !L.wf_item_level.empty()) {
+        const int maxb = Ops<double>::wavefront_max_blocks(s->dim, s->rec, sc->limiter);
+        s->wf_blocks = std::min(std::max(L.wf_max_class_items, 2), maxb);
+        if (s->wf_blocks >= 2) {  // one CTA would never wait: the barrier needs two
+            WfSched &w = s->wf;
+            w.period = L.wf_period;
+            w.nlevels = L.nlevels;
+            w.nitems = (int32_t)L.wf_item_level.size();
+            w.cells = s->upload(L.wf_cells);
+            w.item_ptr = s->upload(L.wf_item_ptr);
+            w.item_level = s->upload(L.wf_item_level);
+            w.lvl_items = s->upload(L.wf_lvl_items);
+            w.ipart = s->dalloc<double>((size_t)2 * w.nitems * 2 * s->nv);
+            w.nacc = L.nlevels / L.wf_period + 3;
+            w.acc = s->dalloc<double>((size_t)w.nacc * 2 * s->nv);
+            w.grec2 = s->dalloc_bytes(Ops<double>::grad_rec_bytes(s->dim) * std::max(L.nint, 1));
+            ck(cudaMemset(w.grec2, 0, Ops<double>::grad_rec_bytes(s->dim) * std::max(L.nint, 1)), "memset");
+            w.sync = s->dalloc<unsigned>(4);
+            s->wf_ready = true;
+        }
+    }
     ck(cudaDeviceSynchronize(), "setup");
     *out = s.release();
     PSST_API_END
@@ -1189,6 +1295,31 @@ extern "C" psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, do
        "norm copy");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
     for (size_t i = 0; i < cnt; ++i) std::memcpy(out + i, &h[i], sizeof(double));
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_use_wavefront(psst_solver *s, int on) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    s->wf_on = on != 0;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_set_wait_limit(psst_solver *s, int64_t ns) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    s->wait_ns = ns < 0 ? psst_solver::kDefaultWaitNs : (uint64_t)ns;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_schedule_info(const psst_solver *s, int64_t *info) {
+    PSST_API_BEGIN
+    if (!s || !info) raise(PSST_ERR_ARG, "psst_solver_schedule_info: null argument");
+    info[0] = wavefront_active(s) ? 1 : 0;
+    info[1] = s->L.wf_period;
+    info[2] = s->L.nlevels;
+    info[3] = (int64_t)s->L.wf_item_level.size();
+    info[4] = s->wf_blocks;
     PSST_API_END
 }
 

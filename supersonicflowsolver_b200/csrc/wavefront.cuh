@@ -1,0 +1,350 @@
+// Sequential LocalAccTime1 as one persistent, cooperative launch per call.
+//
+// The reference evaluates LocalAccTime1 inside its update loop
+// (psstFiniteVolumeGrid.cpp:317-323), so within a stage each cell sees the
+// neighbours updated before it in storage order: a Gauss-Seidel chain.
+// Walking it level by level costs one barrier per level per stage. Here the
+// operations of a whole call (per iteration an optional gradient, then the RK
+// stages) are pipelined as a wavefront: operation m of cell c runs at step
+// P m + level(c) (WfSched in devgrid.hpp), so later operations start on the
+// early levels while earlier ones are still finishing the late levels; a call
+// of n iterations takes P (n ops/iteration - 1) + nlevels + 1 steps instead of
+// n ops/iteration x nlevels. Every value a cell operation computes -- fluxes
+// of its faces (each interior face is computed by both of its cells, with the
+// same arithmetic and so the same bits), the time step from the neighbours
+// the reference's order gives it, the RK update, its ghosts -- is the
+// reference's, bit for bit.
+//
+// Buffers: states by stage parity, gradients by iteration parity, norm
+// partials by operation parity (the schedule keeps every reader of a slot
+// before its next writer). Residual norms are folded per level in level
+// order, so they do not depend on which CTA ran which item.
+//
+// The grid barrier between steps is bounded: a wait longer than wait_ns sets
+// the abort flag and ERR_TIMEOUT, and every CTA leaves at its next barrier.
+#pragma once
+#include "kernels.cuh"
+#include "ops.hpp"
+
+namespace psst {
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier of a cooperative launch (all CTAs co-resident). sync[0]
+// counts arrivals, sync[1] is the generation, sync[2] the abort flag. The
+// last CTA to arrive resets the count and releases the next generation; the
+// others poll it for at most wait_ns (0: not at all). Returns false when the
+// launch is aborted (here or in another CTA).
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned &gen, uint64_t wait_ns, int32_t *err,
+                                             int64_t step) {
+    __shared__ int s_go;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int go = 1;
+        const unsigned g0 = gen;
+        __threadfence();  // this CTA's writes (ordered before by the CTA barrier) before its arrival
+        if (atomicAdd(&sync[0], 1u) == gridDim.x - 1) {
+            sync[0] = 0u;
+            st_release_gpu(&sync[1], g0 + 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            for (;;) {
+                if (ld_acquire_gpu(&sync[1]) != g0) break;
+                if (ld_acquire_gpu(&sync[2]) != 0u) {
+                    go = 0;
+                    break;
+                }
+                if (wait_ns == 0 || global_ns() - t0 > wait_ns) {
+                    atomicExch(&sync[2], 1u);
+                    flag_error(err, ERR_TIMEOUT, (int)step);
+                    go = 0;
+                    break;
+                }
+            }
+        }
+        if (go && ld_acquire_gpu(&sync[2]) != 0u) go = 0;
+        gen = g0 + 1u;
+        s_go = go;
+    }
+    __syncthreads();
+    return s_go != 0;
+}
+
+template <typename R, int NV>
+__device__ __forceinline__ RkIn<NV> rk_load_cg(const DevGrid &g, const DevWork<R> &wk, int first_stage, int32_t c) {
+    RkIn<NV> in;
+    const double *src = first_stage ? wk.w : wk.pw;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.pw[v] = ldcg(src + (int64_t)v * g.nint + c);
+    in.vol = g.V[c];
+    return in;
+}
+
+// Riemann flux with the flux kind chosen at run time (uniform over the launch).
+template <typename R, int DIM, int REC, int LIM>
+__device__ __forceinline__ bool wf_interior_flux(int flux, Prim<R, DIM> r[2], const GradRec<R, DIM> *g0,
+                                                 const GradRec<R, DIM> *g1, const FaceRec<R, DIM> &fr,
+                                                 const R nn[DIM], const Gas &gas, R flow[DIM + 2]) {
+    if (flux == 1) return interior_flux<R, DIM, 1, REC, LIM>(r, g0, g1, fr, nn, gas, flow);
+    if (flux == 2) return interior_flux<R, DIM, 2, REC, LIM>(r, g0, g1, fr, nn, gas, flow);
+    return interior_flux<R, DIM, 3, REC, LIM>(r, g0, g1, fr, nn, gas, flow);
+}
+
+// Gradient operation of iteration k for cell c (psstFiniteVolumeGrid.cpp:307-308).
+template <typename R, int DIM, int REC>
+__device__ __forceinline__ void wf_gradient(const WfArgs<R> &a, int64_t k, int32_t c) {
+    const CellRec<R> *in = a.buf[(a.in_buf + k * a.nst) & 1];
+    GradRec<R, DIM> *out = reinterpret_cast<GradRec<R, DIM> *>(a.gbuf[(a.n_iter - 1 - k) & 1]);
+    if constexpr (REC == 1) {
+        if (a.grad == 1)
+            gradient_cell<R, DIM, 1, 0, true>(a.g, in, out, c);
+        else
+            gradient_cell<R, DIM, 2, 0, true>(a.g, in, out, c);
+    } else if constexpr (REC == 2) {
+        if (a.grad == 1) {
+            if (a.celllim == 4)
+                gradient_cell<R, DIM, 1, 4, true>(a.g, in, out, c);
+            else
+                gradient_cell<R, DIM, 1, 5, true>(a.g, in, out, c);
+        } else {
+            if (a.celllim == 4)
+                gradient_cell<R, DIM, 2, 4, true>(a.g, in, out, c);
+            else
+                gradient_cell<R, DIM, 2, 5, true>(a.g, in, out, c);
+        }
+    }
+}
+
+// RK stage s (stage `stage` of iteration k) for cell c: the fluxes of its
+// faces in the reference's face-loop order (psstConvectiveFlow.cpp:289-299 as
+// a per-cell sum), the time step with the neighbours updated earlier in the
+// reference's order taken from this stage's output
+// (psstLocalTimeCalculation.cpp:90-131), the RK update and primitives
+// (psstFiniteVolumeGrid.cpp:324-346), and the cell's ghosts (:351-366).
+template <typename R, int DIM, int REC, int LIM>
+__device__ __forceinline__ void wf_stage_cell(const WfArgs<R> &a, int64_t s, int64_t k, int stage, int32_t c,
+                                              double sq[DIM + 2], double mx[DIM + 2]) {
+    constexpr int NV = DIM + 2;
+    const DevGrid &g = a.g;
+    const CellRec<R> *in = a.buf[(a.in_buf + s) & 1];
+    CellRec<R> *out = a.buf[(a.in_buf + s + 1) & 1];
+    const GradRec<R, DIM> *gr = reinterpret_cast<const GradRec<R, DIM> *>(a.gbuf[(a.n_iter - 1 - k) & 1]);
+    const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
+    const int first = stage == 0;
+    const RkIn<NV> rin = rk_load_cg<R, NV>(g, a.wk, first, c);
+    R res[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) res[v] = (R)0;
+    const int32_t b = g.csr_ptr[c], e = g.csr_ptr[c + 1];
+    for (int32_t q = b; q < e; ++q) {
+        const int32_t ent = g.csr_ent[q], f = ent >> 1;
+        const FaceRec<R, DIM> fr = ldg(frec + f);
+        R nn[DIM];
+#pragma unroll
+        for (int k2 = 0; k2 < DIM; ++k2) nn[k2] = (R)fr.n[k2];
+        const Prim<R, DIM> p0 = unpack<R, DIM>(ldcg(in + fr.c0));
+        const Prim<R, DIM> p1 = unpack<R, DIM>(ldcg(in + fr.c1));
+        R flow[NV];
+        if (f < g.nfi) {
+            GradRec<R, DIM> g0, g1;
+            if (REC) {
+                g0 = ldcg(gr + fr.c0);
+                g1 = ldcg(gr + fr.c1);
+            }
+            Prim<R, DIM> r[2] = {p0, p1};
+            if (!wf_interior_flux<R, DIM, REC, LIM>(a.flux, r, &g0, &g1, fr, nn, a.gas, flow)) {
+                flag_error(a.wk.err, a.flux == 2 ? ERR_HLL : ERR_HLLC, f);
+#pragma unroll
+                for (int j = 0; j < NV; ++j) flow[j] = (R)0;
+            }
+        } else {
+            boundary_flux<R, DIM>(fr.c0 >= g.nint ? p0 : p1, nn, a.gas, flow);
+        }
+        const R S = (R)fr.S;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const R o = flow[v] * S;  // the face pass's output value
+            if (ent & 1)
+                res[v] += o;
+            else
+                res[v] -= o;
+        }
+    }
+    const Prim<R, DIM> own = unpack<R, DIM>(ldcg(in + c));
+    const double dt = local_time<R, DIM, 1, true, true>(g, in, out, a.gas, a.cfl, 0.0, c, own);
+    const CellRec<R> nrec =
+        rk_update<R, DIM>(g, a.wk, a.gas, rin, dt, a.alpha[stage], first, stage == a.nst - 1, c, res, sq, mx);
+    st16(out + c, nrec);
+    const int32_t gh0 = g.gptr[c], gh1 = g.gptr[c + 1];
+    if (gh1 > gh0) {
+        const Prim<R, DIM> np = unpack<R, DIM>(nrec);
+        for (int32_t i = gh0; i < gh1; ++i) {
+            const int32_t gc = g.nint + i;
+            st16(out + gc, ghost_state<R, DIM>(g, ldcg(in + gc), np, i, a.gas));
+        }
+    }
+}
+
+// Sum of res^2 and max |res| over the cells of one item (fixed pattern: warp
+// trees, then the warps in order), written to out[2 NV]. Whole CTA.
+template <int NV>
+__device__ __forceinline__ void wf_item_partials(double sq[NV], double mx[NV], double *out) {
+    __shared__ double red[2 * NV][kWfBlock / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        double x = sq[v], m = mx[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_down_sync(FULL, x, o);
+            m = fmax(m, __shfl_down_sync(FULL, m, o));
+        }
+        if (lane == 0) {
+            red[v][wid] = x;
+            red[NV + v][wid] = m;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0, m = 0.0;
+        for (int i = 0; i < kWfBlock / 32; ++i) {
+            s += red[threadIdx.x][i];
+            m = fmax(m, red[NV + threadIdx.x][i]);
+        }
+        out[threadIdx.x] = s;
+        out[NV + threadIdx.x] = m;
+    }
+    __syncthreads();  // red is reused by the CTA's next item
+}
+
+// Item i at step T (whole CTA; thread t takes the item's t-th cell).
+template <typename R, int DIM, int REC, int LIM>
+__device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i) {
+    constexpr int NV = DIM + 2;
+    const WfSched &w = a.sc;
+    const int32_t l = w.item_level[i];
+    const int64_t m = (T - l) / w.period;
+    const int j = (int)(m % a.nopi), gofs = a.nopi - a.nst;
+    const int64_t k = m / a.nopi;
+    const int32_t cb = w.item_ptr[i], ce = w.item_ptr[i + 1];
+    const int32_t c = cb + (int32_t)threadIdx.x < ce ? w.cells[cb + threadIdx.x] : -1;
+    if (j < gofs) {  // the iteration's gradient
+        if (c >= 0) wf_gradient<R, DIM, REC>(a, k, c);
+        return;
+    }
+    const int stage = j - gofs;
+    double sq[NV], mx[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
+    if (c >= 0) wf_stage_cell<R, DIM, REC, LIM>(a, k * a.nst + stage, k, stage, c, sq, mx);
+    wf_item_partials<NV>(sq, mx, w.ipart + ((size_t)(m & 1) * w.nitems + i) * 2 * NV);
+}
+
+// Block 0, after the barrier that ends step T: folds the item partials of the
+// levels completed at step T into their stage's running norms, in level order;
+// the last level finishes the stage: RMS and max folded into the iteration's
+// columns as max over stages (the columns of k_norm_finish).
+template <typename R, int NV>
+__device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
+    const WfSched &w = a.sc;
+    const int64_t P = w.period, r = T % P;
+    const int64_t lmax = T < w.nlevels - 1 ? T : (int64_t)w.nlevels - 1;
+    if (lmax < r) return;
+    const int64_t lhi = r + (lmax - r) / P * P;
+    const int64_t t0 = T - P * (a.nops - 1);
+    const int64_t llo = t0 > r ? t0 : r;
+    for (int64_t l = llo + P * (int64_t)threadIdx.x; l <= lhi; l += P * (int64_t)blockDim.x) {
+        const int64_t m = (T - l) / P;
+        const int j = (int)(m % a.nopi), gofs = a.nopi - a.nst;
+        if (j < gofs) continue;  // gradient operation: no residual
+        const int64_t s = (m / a.nopi) * a.nst + (j - gofs);
+        double sum[NV], mx[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sum[v] = mx[v] = 0.0;
+        const double *part = w.ipart + (size_t)(m & 1) * w.nitems * 2 * NV;
+        for (int32_t q = w.lvl_items[2 * l]; q < w.lvl_items[2 * l + 1]; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                sum[v] += ldcg(part + (size_t)q * 2 * NV + v);
+                mx[v] = fmax(mx[v], ldcg(part + (size_t)q * 2 * NV + NV + v));
+            }
+        double *acc = w.acc + (size_t)(s % w.nacc) * 2 * NV;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            if (l == 0) {
+                acc[v] = sum[v];
+                acc[NV + v] = mx[v];
+            } else {
+                acc[v] += sum[v];
+                acc[NV + v] = fmax(acc[NV + v], mx[v]);
+            }
+        }
+        if (l == w.nlevels - 1) {
+            const int64_t it = s / a.nst;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const double rms = sqrt(acc[v] / (double)(a.g.nint > 0 ? a.g.nint : 1));
+                if (rms > a.wk.l2[it * NV + v]) a.wk.l2[it * NV + v] = rms;
+                if (a.wk.linf[it * NV + v] < acc[NV + v]) a.wk.linf[it * NV + v] = acc[NV + v];
+            }
+        }
+    }
+}
+
+template <typename R, int DIM, int REC, int LIM>
+__global__ void __launch_bounds__(kWfBlock, 1) k_wavefront(const __grid_constant__ WfArgs<R> a) {
+    constexpr int NV = DIM + 2;
+    const WfSched &w = a.sc;
+    const int64_t P = w.period;
+    const int64_t tend = P * (a.nops - 1) + w.nlevels + 1;
+    unsigned gen = 0;
+    for (int64_t T = 0; T < tend; ++T) {
+        if (blockIdx.x == 0 && T > 0) wf_fold<R, NV>(a, T - 1);
+        // items of step T: levels l = T (mod P) whose operation (T - l) / P is in [0, nops)
+        const int64_t r = T % P;
+        const int64_t lmax = T < w.nlevels - 1 ? T : (int64_t)w.nlevels - 1;
+        if (lmax >= r) {
+            const int64_t lhi = r + (lmax - r) / P * P;
+            const int64_t t0 = T - P * (a.nops - 1);
+            const int64_t llo = t0 > r ? t0 : r;
+            if (llo <= lhi) {
+                const int32_t i0 = w.lvl_items[2 * llo], i1 = w.lvl_items[2 * lhi + 1];
+                for (int32_t i = i0 + (int32_t)blockIdx.x; i < i1; i += (int32_t)gridDim.x)
+                    wf_item<R, DIM, REC, LIM>(a, T, i);
+            }
+        }
+        if (T + 1 < tend && !grid_barrier(w.sync, gen, a.wait_ns, a.wk.err, T)) return;
+    }
+}
+
+template <typename R, int DIM, int REC, int LIM>
+cudaError_t wf_launch(const WfArgs<R> &a, int nblocks, cudaStream_t s) {
+    void *args[] = {const_cast<WfArgs<R> *>(&a)};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(&k_wavefront<R, DIM, REC, LIM>), dim3(nblocks),
+                                       dim3(kWfBlock), args, 0, s);
+}
+
+template <typename R, int DIM, int REC, int LIM>
+int wf_max_blocks() {
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wavefront<R, DIM, REC, LIM>, kWfBlock, 0) !=
+        cudaSuccess)
+        return 0;
+    return occ * nsm;
+}
+
+}  // namespace psst

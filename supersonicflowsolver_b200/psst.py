@@ -259,6 +259,22 @@ class Solver:
 
     graphs_on = False
 
+    def use_wavefront(self, on=True):
+        """Sequential LocalAccTime1 as one persistent launch per call (default
+        on) or level by level, stage by stage (off); same results."""
+        check(_lib.load().psst_solver_use_wavefront(self._h, int(bool(on))))
+
+    def set_wait_limit(self, nanoseconds):
+        """Bound of each device-side wait of the persistent launch (< 0: default)."""
+        check(_lib.load().psst_solver_set_wait_limit(self._h, int(nanoseconds)))
+
+    def schedule_info(self):
+        """{"wavefront": bool, "period": P, "levels": n, "items": n, "blocks": n}."""
+        out = np.zeros(5, dtype=np.int64)
+        check(_lib.load().psst_solver_schedule_info(self._h, _ptr(out)))
+        return {"wavefront": bool(out[0]), "period": int(out[1]), "levels": int(out[2]), "items": int(out[3]),
+                "blocks": int(out[4])}
+
     def set_active(self, flags):
         """Merged grids: per-case run flags (stopped cases keep their state)."""
         a = np.ascontiguousarray(np.asarray(flags, dtype=np.int32))
@@ -361,7 +377,7 @@ class GridFV:
         self.grid.write_fluent(prim, self.solver.get("rho"), path[:-4] if path.endswith(".sav") else path)
         write_sav(self.grid, prim, iteration, path)
 
-    def explicit_solve(self, chunk=200):
+    def explicit_solve(self, chunk=1000):
         sc = self.scheme
         it = sc.iter
         res_path = os.path.join(self.directory, self._name + "_residual.dat")

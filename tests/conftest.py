@@ -9,7 +9,19 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_DIR = "/root/reference"
+
+def _reference_dir():
+    """The reference checkout (its meshes and shipped outputs), if present:
+    PSST_REFERENCE_DIR, else the directory the build compiled the reference
+    from (noted by __graft_entry__.build), else none."""
+    d = os.environ.get("PSST_REFERENCE_DIR")
+    note = os.path.join(ROOT, "oracle", "_build", "reference_dir")
+    if not d and os.path.exists(note):
+        d = open(note).read().strip()
+    return d if d and os.path.isdir(d) else ""
+
+
+REFERENCE_DIR = _reference_dir()
 
 
 def pytest_configure(config):

@@ -38,6 +38,12 @@ GOLDEN = {
     "g2d_hll_first_order_rk1": ({"kind": "wedge2d", "nx": 40, "ny": 12, "angle_deg": 15.0},
                                 {"flux": 2, "order": 1, "limiter": 3, "grad": 1, "lc": 1, "rk_level": 1,
                                  "cfl": 2.08, "mach": 2.5}, 100),
+    # the reference's 2D case at its own size: 120 x 40 quads (the layout of
+    # its wedge40_120.msh), HLLC, DM + VanLeer, RK4, CFL 0.5, LocalAccTime1 in
+    # its in-loop order, 2000 iterations
+    "g2d_c1_120x40_hllc_dm_vanleer_rk4_2000": ({"kind": "wedge2d", "nx": 120, "ny": 40, "angle_deg": 15.0},
+                                               {"flux": 3, "order": 2, "limiter": 3, "grad": 1, "lc": 1,
+                                                "rk_level": 4, "cfl": 0.5, "mach": 2.5}, 2000),
     # hanging-node mesh: parent cells and faces, quads with five faces
     "g2d_adapted_hllc_lsq_vanleer": ({"kind": "wedge2d_adapted", "nx": 40, "ny": 12, "angle_deg": 15.0,
                                       "refine_frac": 0.2, "seed": 3},

@@ -10,7 +10,6 @@
 import glob
 import json
 import os
-import shutil
 
 import numpy as np
 import pytest
@@ -143,24 +142,23 @@ def _check_vs_reference_files(path, d, name, n):
 
 
 @pytest.mark.slow
-@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE_DIR, "wedge.sav")), reason="reference not mounted")
 def test_oracle_reproduces_shipped_wedge_outputs(tmp_path):
     """wedge80_240.msh + wedge.inp (HLL, 1st order, LocalAccTime1, RK1, CFL 2.08,
     3000 iterations): the shipped wedge.sav byte for byte and every residual
-    column of the shipped wedge_residual.dat."""
-    for f in ("wedge.inp", "wedge.prop", "wedge.par", "wedge.bvp", "wedge.btq"):
-        shutil.copy(os.path.join(REFERENCE_DIR, f), tmp_path / f)
-    with open(os.path.join(REFERENCE_DIR, "wedge80_240.msh"), "rb") as src:
-        (tmp_path / "wedge80_240.msh").write_bytes(src.read().replace(b"\r", b""))
-    o = Oracle(str(tmp_path / "wedge80_240.msh"), str(tmp_path), "wedge")
+    column of the shipped wedge_residual.dat (the reference's files, packed in
+    tests/golden/shipped_wedge)."""
+    import sys
+
+    sys.path.insert(0, GOLDEN_DIR)
+    import make_shipped_wedge
+
+    mesh, sav, res = make_shipped_wedge.unpack(str(tmp_path))
+    o = Oracle(mesh, str(tmp_path), "wedge")
     linf, _ = o.run(3000)
     o.write_sav(str(tmp_path / "wedge.sav"))
-    shipped = open(os.path.join(REFERENCE_DIR, "wedge.sav"), "rb").read().replace(b"\r", b"")
-    assert (tmp_path / "wedge.sav").read_bytes() == shipped
-    rows = [l.split() for l in open(os.path.join(REFERENCE_DIR, "wedge_residual.dat")).read().splitlines() if l.strip()]
-    cols = np.array([[float(x) for x in r[2:]] for r in rows])
+    assert (tmp_path / "wedge.sav").read_bytes() == open(sav, "rb").read()
     printed = np.array([[float("%.3e" % x) for x in row] for row in linf])
-    assert np.array_equal(printed, cols)
+    assert np.array_equal(printed, make_shipped_wedge.residual_columns(res))
 
 
 def test_oracle_extensions_run(tmp_path):
