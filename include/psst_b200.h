@@ -254,8 +254,11 @@ psst_status psst_solver_last_stats(const psst_solver *s, int64_t *launches, doub
  * around every kernel launch, and returns per kernel kind the summed device
  * time (ms) and the launch count. Kinds: 0 gradient (+cell limiter), 1 face
  * pass (fluxes and time-step terms), 2 cell pass (residual, time step, RK
- * update; in the parallel modes also ghosts and norms), 3 ghost update, 4
- * residual-norm finish (the last two only in the sequential mode). */
+ * update; in the parallel modes also ghosts and the norms' block partials;
+ * in the sequential mode's persistent launch the whole call), 3 ghost update
+ * (stage-by-stage sequential mode), 4 residual norms (the parallel modes'
+ * per-iteration reduction, the merged grids' stop rule, the stage-by-stage
+ * sequential mode's per-stage finish). */
 #define PSST_KERNEL_KINDS 5
 psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind, int64_t *launches_per_kind);
 
@@ -328,6 +331,27 @@ psst_status psst_solver_use_graphs(psst_solver *s, int on);
  * run): kernels skip the cells and faces of stopped cases, which keep their
  * state, and their residual columns read 0. */
 psst_status psst_solver_set_active(psst_solver *s, const int32_t *active);
+
+/* Merged grids only; no counterpart in the reference (it runs one case per
+ * process until max_iter). A stop rule evaluated on the device after every
+ * iteration, inside the launch sequence (and so inside a captured graph):
+ * each component of a case's residual column (as psst_solver_case_residuals
+ * returns it) is divided by its maximum over the case's first scale_iters
+ * iterations under the rule -- or by scales[case][dim+2] when scales is not
+ * NULL -- and the case stops at the first iteration where every component is
+ * <= drop, or after caps[case] iterations (caps may be NULL: no cap). A
+ * stopped case is skipped by every later launch, so no case runs past its
+ * stopping iteration whatever the length of the psst_explicit_solve calls.
+ * Setting the rule resets every case's counters and run flags (a case with
+ * cap <= 0 starts stopped); drop <= 0 switches the rule off. */
+psst_status psst_solver_set_stop_rule(psst_solver *s, double drop, int32_t scale_iters, const double *scales,
+                                      const int32_t *caps);
+
+/* Merged grids only. Per case (each argument may be NULL): run flag, iterations
+ * run under the stop rule, iteration at which the drop was reached (0: not
+ * reached), and the normalisation in use [ncase][dim+2]. */
+psst_status psst_solver_case_status(psst_solver *s, int32_t *active, int32_t *iterations, int32_t *converged_at,
+                                    double *scales);
 
 /* Merged grids only. Per-case residual columns of the last psst_explicit_solve
  * call: out[n_iter][ncase][dim+2], each the max over RK stages and the case's

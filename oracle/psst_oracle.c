@@ -64,6 +64,7 @@ struct oracle {
     /* ---- state ---- */
     double *p, *T, *rho, *u, *w, *pw, *res, *dt, *g; /* g: nvol x NG x dim */
     double *u_old, *T_old;                            /* Jacobi snapshot */
+    double *res_conv;                                 /* oracle_convective output */
     /* ---- scheme ---- */
     double M, cp, rm, gamma, cv, ref_vel, CFL;
     long iter, max_iter, iter_step;
@@ -946,6 +947,7 @@ static int setup(oracle_t *o, const char *dir, const char *name) {
     o->w = (double *)calloc((nv + 1) * (dim + 2), sizeof(double));
     o->pw = (double *)calloc((nv + 1) * (dim + 2), sizeof(double));
     o->res = (double *)calloc((nv + 1) * (dim + 2), sizeof(double));
+    o->res_conv = (double *)calloc((nv + 1) * (dim + 2), sizeof(double));
     o->g = (double *)calloc((nv + 1) * NG * dim, sizeof(double));
     o->lim = (double *)calloc((nv + 1) * NG, sizeof(double));
     o->venkat_k = 5.0;
@@ -1528,6 +1530,27 @@ int oracle_run(oracle_t *o, int n_iter, double *res_linf, double *res_l2) {
     return 0;
 }
 
+/* One stage's convective residual of the current state, as the reference
+ * holds it between its face loop (psstConvectiveFlow.cpp:289-299, after the
+ * iteration's gradients, psstFiniteVolumeGrid.cpp:307-311) and the update
+ * loop that consumes and zeroes it (:324-333): copied to res_conv
+ * ("vol_res"); the state and the running residual are left untouched. */
+int oracle_convective(oracle_t *o) {
+    long n = (o->nvol + 1) * (o->dim + 2);
+    if (o->order == 2) {
+        if (o->gradm == 1)
+            gg_calculate(o);
+        else
+            lsq_calculate(o);
+        if (o->limiter >= 4) cell_limiters(o);
+    }
+    memset(o->res, 0, sizeof(double) * n);
+    if (convective(o)) return -1;
+    memcpy(o->res_conv, o->res, sizeof(double) * n);
+    memset(o->res, 0, sizeof(double) * n);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* API                                                                       */
 /* ------------------------------------------------------------------------ */
@@ -1582,6 +1605,7 @@ long oracle_get(const oracle_t *o, const char *name, double *out, long cap) {
     if (!strcmp(name, "vol_w")) COPY(nv * (dim + 2), o->w[i]);
     if (!strcmp(name, "vol_prev_w")) COPY(nv * (dim + 2), o->pw[i]);
     if (!strcmp(name, "vol_dt")) COPY(nv, o->dt[i]);
+    if (!strcmp(name, "vol_res")) COPY(nv * (dim + 2), o->res_conv[i]);
     if (!strcmp(name, "vol_V")) COPY(nv, o->V[i]);
     if (!strcmp(name, "vol_x")) COPY(nv * dim, o->xc[i]);
     if (!strcmp(name, "vol_grad_u")) COPY(nv * dim * dim, o->g[((i / (dim * dim)) * NG + (i % (dim * dim)) / dim) * dim + i % dim]);
@@ -1695,6 +1719,7 @@ void oracle_close(oracle_t *o) {
     free(o->w);
     free(o->pw);
     free(o->res);
+    free(o->res_conv);
     free(o->dt);
     free(o->g);
     free(o->lim);

@@ -47,6 +47,11 @@ int oracle_set(oracle_t *o, const char *key, double value);
  * residual over interior cells. Returns 0, or -1 with oracle_error() set. */
 int oracle_run(oracle_t *o, int n_iter, double *res_linf, double *res_l2);
 
+/* One stage's convective residual of the current state (gradients first for
+ * second order), without updating anything: read it as "vol_res"
+ * [nvol x (dim+2)]. Returns 0, or -1 with oracle_error() set. */
+int oracle_convective(oracle_t *o);
+
 const char *oracle_error(const oracle_t *o);
 int oracle_dim(const oracle_t *o);
 int oracle_nvol(const oracle_t *o);   /* all volumes (interior + ghost), storage order */
@@ -54,7 +59,7 @@ int oracle_nface(const oracle_t *o);  /* all faces of all face zones, map order 
 int oracle_iter(const oracle_t *o);   /* the reference's iter_ counter */
 
 /* Copies a named per-volume / per-face array (layout as oracle/ref_dump.cpp):
- *  vol_p vol_T vol_rho vol_u[dim] vol_w[dim+2] vol_prev_w[dim+2] vol_dt vol_V
+ *  vol_p vol_T vol_rho vol_u[dim] vol_w[dim+2] vol_prev_w[dim+2] vol_dt vol_res[dim+2] vol_V
  *  vol_x[dim] vol_grad_u[dim*dim] vol_grad_p[dim] vol_grad_T[dim]
  *  vol_grad_rho[dim] vol_zone vol_bc vol_boundary
  *  face_S face_n[dim] face_x[dim] face_beta face_zone face_bc face_c0 face_c1

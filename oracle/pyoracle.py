@@ -48,6 +48,7 @@ def lib():
         L.oracle_set_prim.argtypes = [ctypes.c_void_p] * 4
         L.oracle_write_sav.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.oracle_close.argtypes = [ctypes.c_void_p]
+        L.oracle_convective.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -79,6 +80,13 @@ class Oracle:
         if L.oracle_run(self._h, n_iter, linf.ctypes.data, l2.ctypes.data) != 0:
             raise OracleError(L.oracle_error(self._h).decode())
         return linf, l2
+
+    def convective(self):
+        """One stage's convective residual of the current state, (nvol, dim+2)
+        in the reference's component order; the state is not changed."""
+        if lib().oracle_convective(self._h) != 0:
+            raise OracleError(lib().oracle_error(self._h).decode())
+        return self.get("vol_res").reshape(-1, self.nv)
 
     def get(self, name):
         L = lib()

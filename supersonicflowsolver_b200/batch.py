@@ -3,9 +3,12 @@
 The cases' grids are merged into one (psst_grid_merge), so every kernel
 launch advances all of them; each iteration chunk is one CUDA-graph replay
 (psst_solver_use_graphs); launch shapes come from the solver's own tuner
-(psst_solver_autotune); per-case residual columns decide, case by case, when
-the residual drop is reached, and a converged case is stopped
-(psst_solver_set_active) so later launches skip its cells.
+(psst_solver_autotune). The stop rule runs on the device after every
+iteration (psst_solver_set_stop_rule): each case's residual column,
+normalised by its first five iterations, is checked against the drop, and a
+converged (or capped) case is skipped by every later launch, so it stops at
+exactly its converging iteration whatever the chunk length; the host only
+reads the run flags between chunks to see when all cases have stopped.
 
 Workload (seeded): mesh sizes uniform over {60x20, 120x40, 180x60, 240x80}
 quads (x by y), ramp angle U[5, 20] deg, Mach U[1.8, 4.0], p = 101325 Pa,
@@ -23,7 +26,6 @@ import time
 import numpy as np
 
 from . import meshgen
-from .convergence import DropMonitor
 from .psst import Grid, Solver
 
 SIZES = [(60, 20), (120, 40), (180, 60), (240, 80)]
@@ -57,40 +59,32 @@ def build_cases(cases, directory, precision=32, flux=3, limiter=5, cfl=0.5, rk_l
 
 
 def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, caps=None):
-    """Iterates all cases in chunks until every case reaches the residual drop
-    (or max_iter); cells[i] = interior cells of case i; scales[i] (optional) a
-    fixed residual normalisation per case; caps[i] (optional) the iterations
-    case i may run here (it stops unconverged after them). Returns per-case
-    iterations to the drop, the normalisations used, timings and the
-    cell-iterations of running cases."""
+    """Iterates all cases until every case has stopped: at the residual drop,
+    after caps[i] iterations (optional), or after max_iter. cells[i] =
+    interior cells of case i; scales[i] (optional) a fixed residual
+    normalisation per case. The stop rule is evaluated on the device after
+    every iteration, so the counts are exact. Returns per case the iteration
+    of the drop (None: not reached) and the iterations run, the
+    normalisations used, timings and the cell-iterations of running cases."""
     ncase = len(cells)
-    mons = [DropMonitor(drop, scale=None if scales is None else scales[i]) for i in range(ncase)]
-    active = np.ones(ncase, dtype=np.int32)
+    cap = np.full(ncase, max_iter, dtype=np.int64)
     if caps is not None:
-        active[np.asarray(caps) <= 0] = 0
-        if not active.all():
-            solver.set_active(active)
+        cap = np.minimum(cap, np.asarray(caps, dtype=np.int64))
+    solver.set_stop_rule(drop, scale_iters=5, scales=scales, caps=np.maximum(cap, 0))
     done, dev_s = 0, 0.0
-    cells_run = 0
     t0 = time.perf_counter()
-    while done < max_iter and active.any():
+    while done < max_iter and solver.case_status()["active"].any():
         n = min(chunk, max_iter - done)
         solver.explicit_solve(n)
         dev_s += solver.last_stats()[1] / 1000.0
-        cols = solver.case_residuals(n)
         done += n
-        changed = False
-        for i in np.flatnonzero(active):
-            cells_run += int(cells[i]) * n
-            if mons[i].update(cols[:, i, :]) or (caps is not None and done >= caps[i]):
-                active[i] = 0
-                changed = True
-        if changed and active.any():
-            solver.set_active(active)
     wall = time.perf_counter() - t0
-    return {"iterations": [m.converged_at for m in mons], "scales": [m.scale for m in mons], "run": done,
-            "wall_s": wall, "device_s": dev_s,
-            "converged": int(sum(m.converged_at is not None for m in mons)), "cell_iterations": cells_run}
+    st = solver.case_status()
+    ran = st["iterations"].astype(np.int64)
+    return {"iterations": [int(c) if c > 0 else None for c in st["converged_at"]], "ran": ran.tolist(),
+            "scales": st["scales"], "run": done, "wall_s": wall, "device_s": dev_s,
+            "converged": int((st["converged_at"] > 0).sum()),
+            "cell_iterations": int(np.dot(ran, np.asarray(cells, dtype=np.int64)))}
 
 
 def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chunk=100):
@@ -118,7 +112,8 @@ def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chu
     hand = time.perf_counter() - t0
     s32.close()
     # every case keeps the iteration budget of a pure run: max_iter in all
-    caps = [max_iter - (x if x is not None else a["run"]) for x in a["iterations"]]
+    # (a case that did not reach the switch drop ran max_iter in FP32: cap 0)
+    caps = [max_iter - r if x is not None else 0 for x, r in zip(a["iterations"], a["ran"])]
     b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"], caps=caps)
     state = s64.get_state()
     s64.close()

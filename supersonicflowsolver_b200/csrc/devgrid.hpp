@@ -113,8 +113,9 @@ struct DevWork {
     double *dt;          // [nint]
     double *linf;        // [n_iter][dim+2] max over stages and cells of |res|
     double *l2;          // [n_iter][dim+2]
-    double *l2part;      // [nblocks][2][dim+2] per-block sum of res^2 and max |res|
-    unsigned int *ticket;  // [1] blocks finished in the current launch
+    double *l2part;      // [stages][nblocks][2][dim+2] per-block sum of res^2 and max |res|
+    double *l2mid;       // [kNormReduceBlocks][stages][2][dim+2] first level of k_norm_reduce
+    unsigned int *ticket;  // [1] blocks of k_norm_reduce finished in the current launch
     int32_t *err;        // [4] error word, face id, cell id, code
     unsigned long long *case_linf;  // merged grids: [n_iter][ncase][dim+2] max |res| (bits of a
                                     // non-negative double, so integer max = numeric max)
@@ -122,6 +123,21 @@ struct DevWork {
 
 struct Gas {
     double rm, cp, cv, gamma;
+};
+
+// Per-case stop rule of merged grids, evaluated on the device after every
+// iteration: each component of a case's residual column is normalised by its
+// maximum over the case's first scale_iters iterations (or by a given
+// scale); the case stops at the first iteration where every normalised
+// component is <= drop, or when it has run cap iterations.
+struct CaseStop {
+    double drop;
+    int32_t scale_iters;  // 0: the scales are given
+    int32_t *active;      // [ncase] the run flags the kernels read (DevGrid::case_active)
+    int32_t *rows;        // [ncase] iterations run under the rule
+    int32_t *conv_at;     // [ncase] iteration of the drop, 0 while not reached
+    const int32_t *cap;   // [ncase] most iterations a case runs
+    double *scale;        // [ncase][dim+2]
 };
 
 // Wavefront schedule of the sequential LocalAccTime1 (the reference's in-loop

@@ -1001,23 +1001,144 @@ __device__ __forceinline__ void case_max(unsigned long long *cl, int32_t cs, con
     }
 }
 
-// The last block of a launch to finish reduces all partials (no extra launch).
+// Stop rule of merged grids (CaseStop) after one iteration; cl = that
+// iteration's per-case residual columns (bits of non-negative doubles). One
+// thread per case; stopped cases are left as they are.
 template <int NV>
-__device__ __forceinline__ void last_block_finish(const double *part, unsigned *ticket,
-                                                  int32_t nint, double *linf, double *l2, int it_slot) {
-    __shared__ bool is_last;
-    // the threads that wrote this block's partials (block_norm_partials) make
-    // them visible before the block takes its ticket; the other threads' own
-    // stores need no fence
-    if (threadIdx.x < NV) __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (is_last) {
-        __threadfence();
-        finish_norms<NV>(part, gridDim.x, nint, linf, l2, it_slot);
-        if (threadIdx.x == 0) *ticket = 0u;
+__global__ void __launch_bounds__(256) k_case_stop(CaseStop cs, const unsigned long long *cl, int32_t ncase) {
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncase || !cs.active[c]) return;
+    const int32_t rows = ++cs.rows[c];
+    double row[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) row[v] = __longlong_as_double((long long)cl[(int64_t)c * NV + v]);
+    double *sc = cs.scale + (int64_t)c * NV;
+    if (rows <= cs.scale_iters)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sc[v] = rows == 1 ? row[v] : fmax(sc[v], row[v]);
+    if (rows >= cs.scale_iters) {
+        bool done = true;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) done = done && row[v] / (sc[v] > 0.0 ? sc[v] : 1.0) <= cs.drop;
+        if (done) {
+            cs.conv_at[c] = rows;
+            cs.active[c] = 0;
+        }
     }
+    if (cs.active[c] && rows >= cs.cap[c]) cs.active[c] = 0;
+}
+
+// Block partials of the residual norms without a block barrier: each warp
+// reduces its lanes (shuffle trees) into a shared slot, and the last warp of
+// the block to arrive sums the slots in warp order and writes out[2 NV] (sum
+// res^2, max |res|); the other warps leave at once. `count` must be zero at
+// the block's start. FMAX: the maxima are FP32 values, reduced as floats.
+template <int NV, bool FMAX = false>
+__device__ __forceinline__ void lastwarp_partials(double sq[NV], double mx[NV], double *out, unsigned *count) {
+    __shared__ double red[2 * NV][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        double x = sq[v], m = mx[v];
+        float mf = (float)m;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_down_sync(FULL, x, o);
+            if (FMAX)
+                mf = fmaxf(mf, __shfl_down_sync(FULL, mf, o));
+            else
+                m = fmax(m, __shfl_down_sync(FULL, m, o));
+        }
+        if (FMAX) m = (double)mf;
+        if (lane == 0) {
+            red[v][wid] = x;
+            red[NV + v][wid] = m;
+        }
+    }
+    unsigned last = 0;
+    if (lane == 0) {
+        __threadfence_block();
+        last = atomicAdd(count, 1u) == (unsigned)(nw - 1);
+    }
+    if (!__shfl_sync(FULL, last, 0)) return;
+    __threadfence_block();
+    if (lane < 2 * NV) {
+        const volatile double *r = red[lane];
+        double a = 0.0;
+        for (int i = 0; i < nw; ++i) a = lane < NV ? a + r[i] : fmax(a, r[i]);
+        out[lane] = a;
+    }
+}
+
+// Residual columns of one iteration from the cell pass's block partials of
+// its nstage stages (part[stage][nblk][2 NV]): per stage the RMS over the
+// interior cells and the max |res|, then the max over stages (the reference's
+// column is max over stages and cells, psstFiniteVolumeGrid.cpp:331-332; the
+// RMS column is this project's). Block g reduces a fixed range of partials of
+// every stage into mid[g][stage]; the last block to finish combines them in
+// block order (reproducible for a given nblk and grid).
+template <int NV>
+__global__ void __launch_bounds__(256) k_norm_reduce(const double *part, int nblk, int nstage, int32_t nint,
+                                                     double *mid, unsigned *ticket, double *linf, double *l2,
+                                                     int it_slot) {
+    __shared__ double red[2 * NV][8];
+    __shared__ bool is_last;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int chunk = (nblk + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int b0 = (int)blockIdx.x * chunk, b1 = min(nblk, b0 + chunk);
+    for (int st = 0; st < nstage; ++st) {
+        double s[NV], m[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] = m[v] = 0.0;
+        const double *p = part + (int64_t)st * nblk * 2 * NV;
+        for (int b = b0 + t; b < b1; b += blockDim.x)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                s[v] += p[(int64_t)b * 2 * NV + v];
+                m[v] = fmax(m[v], p[(int64_t)b * 2 * NV + NV + v]);
+            }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                s[v] += __shfl_down_sync(FULL, s[v], o);
+                m[v] = fmax(m[v], __shfl_down_sync(FULL, m[v], o));
+            }
+            if (lane == 0) {
+                red[v][wid] = s[v];
+                red[NV + v][wid] = m[v];
+            }
+        }
+        __syncthreads();
+        if (t < 2 * NV) {
+            double a = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) a = t < NV ? a + red[t][i] : fmax(a, red[t][i]);
+            mid[((int64_t)blockIdx.x * nstage + st) * 2 * NV + t] = a;
+        }
+        __syncthreads();
+    }
+    if (t < 2 * NV) __threadfence();
+    __syncthreads();
+    if (t == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    if (t < NV) {
+        double rms = 0.0, mx = 0.0;
+        for (int st = 0; st < nstage; ++st) {
+            double a = 0.0;
+            for (int g = 0; g < (int)gridDim.x; ++g) {
+                const double *q = mid + ((int64_t)g * nstage + st) * 2 * NV;
+                a += q[t];
+                mx = fmax(mx, q[NV + t]);
+            }
+            const double r = sqrt(a / (double)(nint > 0 ? nint : 1));
+            if (r > rms) rms = r;
+        }
+        l2[it_slot * NV + t] = rms;
+        linf[it_slot * NV + t] = mx;
+    }
+    if (t == 0) *ticket = 0u;
 }
 
 
@@ -1044,7 +1165,9 @@ __device__ __forceinline__ void gather_residual(const DevGrid &g, const FaceOut<
 // the scatter at psstConvectiveFlow.cpp:289-299), local time step from the
 // faces' terms in the cell's own face order (the reference's accumulation
 // order, psstLocalTimeCalculation.cpp:117-127, 189-203), RK update, the cell's
-// ghost cells, block norm partials; the last block finishes the stage norms.
+// ghost cells, and the block's norm partials for this stage (formed by the
+// block's last warp to finish, so no warp waits at a block barrier;
+// k_norm_reduce turns the stages' partials into the iteration's columns).
 // At least 4 blocks of 256 per SM (64 registers): the pass is bound by the
 // latency of its gathers, and the occupancy gained outweighs a 24-byte spill
 // (0.61 -> 0.56 ms per launch on 6M tets, FP32).
@@ -1071,12 +1194,15 @@ __device__ __forceinline__ R lc1_normal_velocities(const FaceOut<R, DIM> &o, int
 template <typename R, int DIM, int LC, bool BATCH>
 __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
                                               double cfl, double dt_uniform, double alpha, int stage,
-                                              int it_slot) {
-    // stage: bit 0 first stage of the iteration, bit 1 last stage
+                                              int kstage, int it_slot) {
+    // stage: bit 0 first stage of the iteration, bit 1 last stage; kstage: its index
     using FO = FaceOut<R, DIM>;
     const int first_stage = stage & 1;
     constexpr int NV = DIM + 2;
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ unsigned warps_done;  // lastwarp_partials
+    if (threadIdx.x == 0) warps_done = 0u;
+    __syncthreads();
     double sq[NV], mx[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
@@ -1186,8 +1312,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
         }
     }
     if (BATCH) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, run ? g.cell_case[c] : -1, mx);
-    block_norm_partials<NV, sizeof(R) == 4>(sq, mx, wk.l2part);
-    last_block_finish<NV>(wk.l2part, wk.ticket, g.nint, wk.linf, wk.l2, it_slot);
+    lastwarp_partials<NV, sizeof(R) == 4>(sq, mx, wk.l2part + ((int64_t)kstage * gridDim.x + blockIdx.x) * 2 * NV,
+                                          &warps_done);
 }
 
 // Thread-per-cell update reading the face outputs (GATHER) or the residual of

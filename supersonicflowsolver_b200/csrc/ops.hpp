@@ -12,6 +12,7 @@ namespace psst {
 constexpr int kBlock = 256;
 constexpr int kMinBlock = 64;  // smallest launch shape the tuner may pick
 constexpr int kWfBlock = 128;  // threads per CTA of k_wavefront (and cells per work item)
+constexpr int kNormReduceBlocks = 64;  // blocks of k_norm_reduce (first level of its two-level sum)
 inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
 template <typename R>
@@ -39,10 +40,13 @@ struct Ops {
     static void face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st,
                      const DevWork<R> &wk, const Gas &gas, cudaStream_t s);
     // cell pass of the parallel modes (lc 0, 2, 1 from stage-start values):
-    // residual, time step, RK update, ghosts, norms (last block finishes them)
+    // residual, time step, RK update, ghosts, block norm partials of stage kstage
     static void cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                      const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
-                     int stage, int it_slot, cudaStream_t s);  // stage: 1 first, 2 last (bits)
+                     int stage, int kstage, int it_slot, cudaStream_t s);  // stage: 1 first, 2 last (bits)
+    // the iteration's residual columns from the cell passes' partials of nstage stages
+    static void norm_reduce(int dim, const DevGrid &g, const DevWork<R> &wk, int nstage, int it_slot,
+                            cudaStream_t s);
     static void residual(int dim, const DevGrid &g, const DevWork<R> &wk, cudaStream_t s);
     // cell update from face outputs (gather) or from wk.res; seq: the
     // sequential LocalAccTime1 (single block over levels); norms by norm_finish
@@ -52,6 +56,9 @@ struct Ops {
     static void ghost_update(int dim, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                              const Gas &gas, cudaStream_t s);
     static void norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, int it_slot, cudaStream_t s);
+    // merged grids: the per-case stop rule after iteration it_slot
+    static void case_stop(int dim, const DevGrid &g, const DevWork<R> &wk, const CaseStop &cs, int it_slot,
+                          cudaStream_t s);
     // Sequential LocalAccTime1 over a whole call as one cooperative launch of
     // nblocks CTAs (k_wavefront; FP64 only, cudaErrorNotSupported otherwise).
     static cudaError_t wavefront(int dim, int rec, int lim, const WfArgs<R> &a, int nblocks, cudaStream_t s);

@@ -1,6 +1,8 @@
 // Launcher bodies for Ops<R>: template dispatch from runtime scheme options to
 // kernel instantiations. Included by kernels_f64.cu / kernels_f32.cu only.
 #pragma once
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "ops.hpp"
 #include "wavefront.cuh"
@@ -140,34 +142,46 @@ void Ops<R>::face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g,
 // ---- cell pass (parallel modes) ----
 template <typename R, int DIM>
 static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const DevWork<R> &wk,
-                   const Gas &gas, double cfl, double dtu, double alpha, int first, int it, cudaStream_t s) {
+                   const Gas &gas, double cfl, double dtu, double alpha, int first, int ks, int it, cudaStream_t s) {
     const int bs = g.blk_cell, nb = nblocks(g.nint, bs);
     if (g.cell_case) {  // merged grids: per-case run flags and residual columns
         if (lc == 1)
-            k_cell<R, DIM, 1, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+            k_cell<R, DIM, 1, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         else if (lc == 2)
-            k_cell<R, DIM, 2, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+            k_cell<R, DIM, 2, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         else
-            k_cell<R, DIM, 0, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+            k_cell<R, DIM, 0, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         return;
     }
     if (lc == 1)
-        k_cell<R, DIM, 1, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 1, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
     else if (lc == 2)
-        k_cell<R, DIM, 2, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 2, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
     else
-        k_cell<R, DIM, 0, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, it);
+        k_cell<R, DIM, 0, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
 }
 
 template <typename R>
 void Ops<R>::cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                   const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha, int stage,
-                  int it_slot, cudaStream_t s) {
+                  int kstage, int it_slot, cudaStream_t s) {
     if (g.nint == 0) return;
     if (dim == 2)
-        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, it_slot, s);
+        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, s);
     else
-        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, it_slot, s);
+        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, s);
+}
+
+template <typename R>
+void Ops<R>::norm_reduce(int dim, const DevGrid &g, const DevWork<R> &wk, int nstage, int it_slot, cudaStream_t s) {
+    if (g.nint == 0) return;
+    const int nblk = nblocks(g.nint, g.blk_cell), grid = std::min(nblk, kNormReduceBlocks);
+    if (dim == 2)
+        k_norm_reduce<4><<<grid, 256, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
+                                              it_slot);
+    else
+        k_norm_reduce<5><<<grid, 256, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
+                                              it_slot);
 }
 
 template <typename R>
@@ -233,6 +247,16 @@ void Ops<R>::norm_finish(int dim, const DevWork<R> &wk, int nblk, int32_t nint, 
         k_norm_finish<4><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
     else
         k_norm_finish<5><<<1, 256, 0, s>>>(wk.l2part, nblk, nint, wk.linf, wk.l2, it_slot);
+}
+
+template <typename R>
+void Ops<R>::case_stop(int dim, const DevGrid &g, const DevWork<R> &wk, const CaseStop &cs, int it_slot,
+                       cudaStream_t s) {
+    const unsigned long long *cl = wk.case_linf + (int64_t)it_slot * g.ncase * (dim + 2);
+    if (dim == 2)
+        k_case_stop<4><<<nblocks(g.ncase), kBlock, 0, s>>>(cs, cl, g.ncase);
+    else
+        k_case_stop<5><<<nblocks(g.ncase), kBlock, 0, s>>>(cs, cl, g.ncase);
 }
 
 // ---- sequential LocalAccTime1 as one persistent launch (FP64 only) ----

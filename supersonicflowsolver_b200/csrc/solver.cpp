@@ -21,6 +21,7 @@
 // carry a per-cell case id, per-case run flags and per-case residual columns.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -447,6 +448,9 @@ struct psst_solver {
     // sequential LocalAccTime1 as one persistent launch per call (FP64, single
     // grids): schedule uploaded (wf_ready), switched on (wf_on), CTAs, and the
     // bound of every grid-barrier wait
+    // merged grids: the per-case stop rule evaluated on the device (CaseStop)
+    bool stop_on = false;
+    CaseStop stop{};
     bool wf_ready = false, wf_on = true;
     WfSched wf{};
     int wf_blocks = 0;
@@ -535,8 +539,9 @@ void alloc_state(psst_solver *s, const psst_grid &G) {
     w.fout = s->dalloc_bytes(Ops<R>::face_out_bytes(dim) * std::max(nface, 1));
     w.res = s->dalloc<R>((size_t)nv * nint);
     w.dt = s->dalloc<double>(nint);
-    // sized for the smallest cell-pass block (64 threads): one partial per block
-    w.l2part = s->dalloc<double>((size_t)2 * nv * std::max(nblocks(nint, kMinBlock), 1));
+    // sized for the smallest cell-pass block (64 threads): one partial per block and RK stage
+    w.l2part = s->dalloc<double>((size_t)2 * nv * std::max(nblocks(nint, kMinBlock), 1) * s->sc.rk_level);
+    w.l2mid = s->dalloc<double>((size_t)2 * nv * kNormReduceBlocks * s->sc.rk_level);
     w.ticket = s->dalloc<unsigned int>(1);
     w.err = s->dalloc<int32_t>(4);
     ck(cudaMemset(w.grec, 0, gbytes * std::max(nint, 1)), "memset");
@@ -625,9 +630,13 @@ void one_stage(psst_solver *s, int k, int it_slot, bool gather, Mark &&mark) {
     }
     if (gather && !s->seq) {
         const int stage = (k == 0 ? 1 : 0) | (k == s->sc.rk_level - 1 ? 2 : 0);
-        Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], stage,
+        Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], stage, k,
                      it_slot, s->stream);
         mark(K_CELL);
+        if (k == s->sc.rk_level - 1) {  // the iteration's residual columns
+            Ops<R>::norm_reduce(s->dim, s->g, w, s->sc.rk_level, it_slot, s->stream);
+            mark(K_NORM);
+        }
     } else {
         Ops<R>::cell_update(s->dim, s->sc.lc, s->seq, gather, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform,
                             s->sc.rk[k], k == 0, s->stream);
@@ -687,6 +696,10 @@ void iterations(psst_solver *s, int n_iter, Mark &&mark) {
             mark(K_GRADIENT);
         }
         for (int k = 0; k < s->sc.rk_level; ++k) one_stage<R>(s, k, it, true, mark);
+        if (s->stop_on) {
+            Ops<R>::case_stop(s->dim, s->g, w, s->stop, it, s->stream);
+            mark(K_NORM);
+        }
     }
 }
 
@@ -1278,6 +1291,75 @@ extern "C" psst_status psst_solver_set_active(psst_solver *s, const int32_t *act
                        cudaMemcpyHostToDevice, s->stream),
        "flags upload");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_set_stop_rule(psst_solver *s, double drop, int32_t scale_iters,
+                                                 const double *scales, const int32_t *caps) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (s->L.cell_case.empty()) raise(PSST_ERR_ARG, "psst_solver_set_stop_rule: the grid is not a merged grid");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    s->drop_graphs();  // the launch sequence changes
+    const int32_t nc = s->L.ncase;
+    if (!(drop > 0.0)) {
+        s->stop_on = false;
+        return PSST_OK;
+    }
+    if (!scales && scale_iters < 1) raise(PSST_ERR_ARG, "scale_iters must be >= 1 without given scales");
+    if (!s->stop.rows) {
+        s->stop.rows = s->dalloc<int32_t>(nc);
+        s->stop.conv_at = s->dalloc<int32_t>(nc);
+        s->stop.cap = s->dalloc<int32_t>(nc);
+        s->stop.scale = s->dalloc<double>((size_t)nc * s->nv);
+    }
+    s->stop.drop = drop;
+    s->stop.scale_iters = scales ? 0 : scale_iters;
+    s->stop.active = const_cast<int32_t *>(s->g.case_active);
+    std::vector<int32_t> cap(nc, INT32_MAX), zero(nc, 0);
+    if (caps)
+        for (int32_t i = 0; i < nc; ++i) cap[i] = caps[i];
+    std::vector<double> sc((size_t)nc * s->nv, 0.0);
+    if (scales) std::copy(scales, scales + (size_t)nc * s->nv, sc.begin());
+    for (int32_t i = 0; i < nc; ++i) s->active_h[i] = cap[i] > 0 ? 1 : 0;
+    ck(cudaMemcpyAsync(const_cast<int32_t *>(s->stop.cap), cap.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       s->stream),
+       "copy");
+    ck(cudaMemcpyAsync(s->stop.rows, zero.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream), "copy");
+    ck(cudaMemcpyAsync(s->stop.conv_at, zero.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream),
+       "copy");
+    ck(cudaMemcpyAsync(s->stop.scale, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "copy");
+    ck(cudaMemcpyAsync((void *)s->g.case_active, s->active_h.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       s->stream),
+       "copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    s->stop_on = true;
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_case_status(psst_solver *s, int32_t *active, int32_t *iterations,
+                                               int32_t *converged_at, double *scales) {
+    PSST_API_BEGIN
+    if (!s) raise(PSST_ERR_ARG, "null solver");
+    if (s->L.cell_case.empty()) raise(PSST_ERR_ARG, "psst_solver_case_status: the grid is not a merged grid");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    const int32_t nc = s->L.ncase;
+    auto get = [&](void *dst, const void *src, size_t bytes) {
+        if (dst && src) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream), "copy");
+    };
+    get(active, s->g.case_active, nc * sizeof(int32_t));
+    get(iterations, s->stop.rows, nc * sizeof(int32_t));
+    get(converged_at, s->stop.conv_at, nc * sizeof(int32_t));
+    get(scales, s->stop.scale, (size_t)nc * s->nv * sizeof(double));
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    if (!s->stop.rows) {  // no rule set yet: nothing run under it
+        if (iterations) std::fill(iterations, iterations + nc, 0);
+        if (converged_at) std::fill(converged_at, converged_at + nc, 0);
+        if (scales) std::fill(scales, scales + (size_t)nc * s->nv, 0.0);
+    }
+    if (active)
+        for (int32_t i = 0; i < nc; ++i) s->active_h[i] = active[i];
     PSST_API_END
 }
 

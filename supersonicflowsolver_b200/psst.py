@@ -288,6 +288,25 @@ class Solver:
         check(_lib.load().psst_solver_case_residuals(self._h, int(n_iter), _ptr(out)))
         return out
 
+    def set_stop_rule(self, drop, scale_iters=5, scales=None, caps=None):
+        """Merged grids: the per-case stop rule evaluated on the device after
+        every iteration (drop <= 0 switches it off); see psst_solver_set_stop_rule."""
+        ncase = len(self.grid.cases()) - 1
+        sc = None if scales is None else np.ascontiguousarray(np.asarray(scales, dtype=np.float64).reshape(ncase, self.nv))
+        cp = None if caps is None else np.ascontiguousarray(np.asarray(caps, dtype=np.int32).reshape(ncase))
+        check(_lib.load().psst_solver_set_stop_rule(self._h, float(drop), int(scale_iters),
+                                                    None if sc is None else _ptr(sc), None if cp is None else _ptr(cp)))
+
+    def case_status(self):
+        """Merged grids: {"active", "iterations", "converged_at", "scales"} per case."""
+        ncase = len(self.grid.cases()) - 1
+        act = np.zeros(ncase, dtype=np.int32)
+        its = np.zeros(ncase, dtype=np.int32)
+        conv = np.zeros(ncase, dtype=np.int32)
+        sc = np.zeros((ncase, self.nv))
+        check(_lib.load().psst_solver_case_status(self._h, _ptr(act), _ptr(its), _ptr(conv), _ptr(sc)))
+        return {"active": act, "iterations": its, "converged_at": conv, "scales": sc}
+
     def set_stream(self, stream_ptr):
         check(_lib.load().psst_solver_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 

@@ -166,3 +166,43 @@ def test_mixed_precision_batch_reaches_the_fp64_field(tmp_path):
     assert p["converged"] == len(cases)
     e = field_error(r["state"], s.get_state(), merged)
     assert all(e[k]["rms_rel"] < 1e-5 for k in e), e
+
+
+@pytest.mark.gpu
+def test_device_stop_rule_stops_each_case_at_its_own_iteration(tmp_path):
+    """The stop rule runs on the device after every iteration: each case stops
+    at exactly the iteration where its normalised residual column first drops
+    below the threshold (as DropMonitor finds it on the case run alone), or at
+    its cap, whatever the chunk length of the calls; a stopped case keeps the
+    state it had at that iteration."""
+    from supersonicflowsolver_b200.convergence import DropMonitor
+
+    cases = [(12, 4, 10.0, 2.5), (16, 6, 15.0, 3.0), (10, 4, 8.0, 2.2)]
+    grids, schemes, prims, m = build(tmp_path, cases=cases, flux=2, order=1, cfl=0.8, rk_level=1)
+    drop, caps = 0.05, [3000, 3000, 7]
+    solo_at, solo_state = [], []
+    for i, (g, sc, prim) in enumerate(zip(grids, schemes, prims)):
+        s = Solver(g, sc)
+        s.set_state(prim)
+        mon = DropMonitor(drop)
+        states = {}
+        for it in range(1, caps[i] + 1):
+            linf, _ = s.explicit_solve(1)
+            states[it] = s.get_state()
+            if mon.update(linf):
+                break
+        solo_at.append(mon.converged_at)
+        solo_state.append(states[mon.converged_at or caps[i]])
+    assert solo_at[0] is not None and solo_at[1] is not None and solo_at[2] is None
+    b = Solver(m, schemes[0])
+    b.set_state(m.initial_state())
+    b.use_graphs(True)
+    b.set_stop_rule(drop, scale_iters=5, caps=caps)
+    while b.case_status()["active"].any():
+        b.explicit_solve(13)
+    st = b.case_status()
+    assert list(st["converged_at"]) == [solo_at[0], solo_at[1], 0]
+    assert list(st["iterations"]) == [solo_at[0], solo_at[1], caps[2]]
+    state = b.get_state()
+    for i in range(3):
+        assert np.array_equal(case_part(state, m, i, 4), solo_state[i]), "case %d" % i

@@ -161,6 +161,27 @@ def test_oracle_reproduces_shipped_wedge_outputs(tmp_path):
     assert np.array_equal(printed, make_shipped_wedge.residual_columns(res))
 
 
+@pytest.mark.parametrize("ckw", [dict(flux=2, order=1, lc=1, rk_level=1), dict(flux=3, order=2, limiter=3, lc=2,
+                                                                               rk_level=1)],
+                         ids=["hll_first", "hllc_vanleer"])
+def test_oracle_residual_is_the_one_its_update_consumes(tmp_path, ckw):
+    """The exported one-stage residual ("vol_res") is the residual the pinned
+    update consumes: after one RK1 iteration, w = prev_w - dt*a*res/V bit for
+    bit (psstFiniteVolumeGrid.cpp:324-330) for every interior cell."""
+    mesh = meshgen.wedge2d(30, 10, 15.0, jitter=0.15, shuffle_seed=1)
+    path, d, name = make_case(tmp_path, mesh, max_iter=2, **ckw)
+    o = Oracle(path, d, name)
+    o.run(1)
+    res = o.convective()
+    w0 = o.get("vol_w").reshape(-1, 4)
+    o.run(1)
+    interior = o.get("vol_bc") == 1
+    dt, V = o.get("vol_dt")[interior], o.get("vol_V")[interior]
+    w1 = o.get("vol_w").reshape(-1, 4)[interior]
+    expect = w0[interior] - dt[:, None] * 1.0 * res[interior] / V[:, None]
+    assert np.array_equal(w1, expect)
+
+
 def test_oracle_extensions_run(tmp_path):
     """Limiters 4/5 and the Jacobi LocalAccTime1 (no reference counterpart)
     stay finite and differ from the sequential evaluation only slightly."""

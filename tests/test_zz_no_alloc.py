@@ -1,6 +1,8 @@
 """psst_convective_residual_static: the residual entry point that allocates no
 memory, checked through the C ABI against the solver's own residual
-(psst_convective_calculate with first-order reconstruction).
+(psst_convective_calculate with first-order reconstruction) and against the
+oracle's residual of the same state (the reference's face loop,
+psstConvectiveFlow.cpp:289-299).
 
 Callers that cannot allocate device memory -- code under an application or
 framework that owns every device allocation, or an embedded solver whose host
@@ -16,6 +18,7 @@ import numpy as np
 import pytest
 
 from conftest import make_case
+from oracle.pyoracle import Oracle
 from supersonicflowsolver_b200 import _lib, meshgen
 from supersonicflowsolver_b200.psst import Grid, PsstError, Solver
 
@@ -81,13 +84,16 @@ def test_static_residual_matches_solver_twice(tmp_path, mesh, flux):
                "n": g.get("face_n").reshape(g.nface, g.dim).T.copy(), "ptr": ptr, "ent": ent}
     s = Solver(g, sc, device=0)
     s.set_state(prim)
+    o = Oracle(path, d, name)
     for call in range(2):  # two calls in a row, on two different states
         s.explicit_solve(1)
+        o.run(1)
         s.convective_calculate()
         expect = s.get("residual").reshape(g.nvol, g.dim + 2)[:nint]
         got = _call(g, sc, _prim_soa(s, g, sc), tensors, torch)
         assert np.all(np.isfinite(got))
         assert np.array_equal(got, expect), "call %d" % (call + 1)
+        assert np.array_equal(got, o.convective()[:nint]), "call %d vs the oracle" % (call + 1)
 
 
 def test_static_residual_rejects_meshes_above_its_buffer():
