@@ -212,6 +212,20 @@ psst_status psst_solver_set_state(psst_solver *s, const double *prim);
  * state w[(dim+2)*nvol] (rho*u.., rho, rho*E; zero for ghosts). */
 psst_status psst_solver_get_state(psst_solver *s, double *prim, double *w);
 
+/* Binary checkpoint, next to the reference's .sav (psstFiniteVolumeGrid.cpp:
+ * 606-639, read back at :559-604). The .sav keeps 11 decimals of p, T, u and
+ * the restart recomputes rho and w, so a run resumed from it does not continue
+ * exactly. The checkpoint holds, at full precision, the primitive records (p,
+ * T, rho, u..) of every volume as the solver holds them, the FP64 conservative
+ * state w and the iteration counter: N iterations, save, load into a solver
+ * of the same grid, scheme and precision, M iterations equals N + M
+ * iterations bit for bit. Format (native byte order): "PSSTCKP1", int32 dim,
+ * int32 precision, int64 nvol, nint, iter; then doubles prim[(2+dim)*nvol]
+ * (layout of psst_solver_get_state), rho[nvol], w[nvol*(dim+2)]. Loading
+ * checks grid size and precision (PSST_ERR_FORMAT otherwise). */
+psst_status psst_solver_save_checkpoint(psst_solver *s, const char *path);
+psst_status psst_solver_load_checkpoint(psst_solver *s, const char *path);
+
 /* psstInterfaceGradientCalc::calculate (psstGradCalculation.h:20;
  * psstGreenGauss .cpp:80-177, psstLeastSquare .cpp:268-368). For limiters 4/5
  * this also evaluates the cell limiter. */

@@ -29,7 +29,8 @@ EXPORTED = [
     "psst_grid_merge", "psst_grid_case_count", "psst_grid_initial_state", "psst_write_fluent",
     "psst_solver_use_graphs", "psst_solver_set_active", "psst_solver_case_residuals",
     "psst_solver_use_wavefront", "psst_solver_set_wait_limit", "psst_solver_schedule_info",
-    "psst_solver_set_stop_rule", "psst_solver_case_status",
+    "psst_solver_set_stop_rule", "psst_solver_case_status", "psst_solver_save_checkpoint",
+    "psst_solver_load_checkpoint",
     "psst_mlp_create", "psst_mlp_param_count", "psst_mlp_get_params", "psst_mlp_set_params", "psst_mlp_forward",
     "psst_mlp_gradients", "psst_mlp_train_step", "psst_mlp_set_stream", "psst_mlp_destroy", "psst_tc_gemm_bf16",
 ]
@@ -128,6 +129,8 @@ def load():
         "psst_solver_schedule_info": (I, [P, P]),
         "psst_solver_set_stop_rule": (I, [P, D, ctypes.c_int32, P, P]),
         "psst_solver_case_status": (I, [P, P, P, P, P]),
+        "psst_solver_save_checkpoint": (I, [P, S]),
+        "psst_solver_load_checkpoint": (I, [P, S]),
         "psst_mlp_create": (I, [I, ctypes.c_uint64, ctypes.POINTER(P)]),
         "psst_mlp_param_count": (I64, [P]),
         "psst_mlp_get_params": (I, [P, P, I64]),

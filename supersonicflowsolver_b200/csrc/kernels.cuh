@@ -1415,6 +1415,24 @@ __global__ void k_gather_prim(int32_t nall, DevState<R> st, const double *prim, 
     st16(st.rec + d, r);
 }
 
+// Exact state from a checkpoint: records (p, T, rho, u..) of every volume and
+// the FP64 conservative state w of interior cells, as stored (no prologue:
+// rho and w are not recomputed, so a resumed run continues bit for bit).
+template <typename R, int DIM>
+__global__ void k_set_exact(int32_t nall, int32_t nint, DevState<R> st, double *wdev, const double *prim,
+                            const double *rho, const double *w, const int32_t *vol, int64_t nvol) {
+    const int32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nall) return;
+    const int64_t v = vol[d];
+    R u[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) u[k] = (R)prim[(2 + k) * nvol + v];
+    st16(st.rec + d, pack<R, DIM>((R)prim[v], (R)prim[nvol + v], (R)rho[v], u));
+    if (d < nint)
+#pragma unroll
+        for (int q = 0; q < DIM + 2; ++q) wdev[(int64_t)q * nint + d] = w[v * (DIM + 2) + q];
+}
+
 template <typename R, int DIM>
 __global__ void k_scatter_prim(int32_t nall, DevState<R> st, double *prim, const int32_t *vol, int64_t nvol) {
     const int32_t d = blockIdx.x * blockDim.x + threadIdx.x;

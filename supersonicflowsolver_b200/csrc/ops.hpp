@@ -29,6 +29,10 @@ struct Ops {
                             const int32_t *vol, int64_t nvol, cudaStream_t s);
     static void scatter_prim(int dim, const DevGrid &g, const DevState<R> &st, double *prim, const int32_t *vol,
                              int64_t nvol, cudaStream_t s);
+    // exact state (records incl. rho, and w) from reference-ordered FP64 arrays
+    static void set_exact(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
+                          const double *prim, const double *rho, const double *w, const int32_t *vol, int64_t nvol,
+                          cudaStream_t s);
     // w[v][dim+2] per volume (interior cells only)
     static void scatter_w(int dim, const DevGrid &g, const DevWork<R> &wk, double *w, const int32_t *vol,
                           cudaStream_t s);

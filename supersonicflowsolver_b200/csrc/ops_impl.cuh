@@ -53,6 +53,16 @@ void Ops<R>::scatter_prim(int dim, const DevGrid &g, const DevState<R> &st, doub
 }
 
 template <typename R>
+void Ops<R>::set_exact(int dim, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const double *prim,
+                       const double *rho, const double *w, const int32_t *vol, int64_t nvol, cudaStream_t s) {
+    if (g.nall == 0) return;
+    if (dim == 2)
+        k_set_exact<R, 2><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, g.nint, st, wk.w, prim, rho, w, vol, nvol);
+    else
+        k_set_exact<R, 3><<<nblocks(g.nall), kBlock, 0, s>>>(g.nall, g.nint, st, wk.w, prim, rho, w, vol, nvol);
+}
+
+template <typename R>
 void Ops<R>::scatter_w(int dim, const DevGrid &g, const DevWork<R> &wk, double *w, const int32_t *vol,
                        cudaStream_t s) {
     if (g.nint == 0) return;

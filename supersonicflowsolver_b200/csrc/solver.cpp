@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -435,7 +436,7 @@ struct psst_solver {
     int norm_cap = 0;
     int last_n = 0;                    // iterations of the last psst_explicit_solve
     int32_t *d_vol = nullptr;          // reference volume of each device cell
-    double *d_prim = nullptr, *d_w = nullptr;  // reference-ordered state staging
+    double *d_prim = nullptr, *d_w = nullptr, *d_rho = nullptr;  // reference-ordered state staging
     std::vector<int32_t> active_h;     // merged grids: per-case run flags (host copy)
     // pinned host staging of a call's residual columns and error word: one
     // stream synchronisation per call, no pageable-memory copies
@@ -881,6 +882,7 @@ void ensure_staging(psst_solver *s) {
     s->d_vol = s->upload(vol);
     s->d_prim = s->dalloc<double>((size_t)(2 + s->dim) * s->nvol_ref);
     s->d_w = s->dalloc<double>((size_t)s->nv * s->nvol_ref);
+    s->d_rho = s->dalloc<double>((size_t)s->nvol_ref);
 }
 
 template <typename R>
@@ -913,6 +915,79 @@ void get_state(psst_solver *s, double *prim, double *wout) {
     }
     ck(cudaGetLastError(), "state scatter");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
+}
+
+// Binary checkpoint: everything an iteration boundary carries, at full
+// precision -- the primitive records (p, T, rho, u..) of every volume as the
+// solver holds them and the FP64 conservative state w -- plus the iteration
+// counter. (The reference's .sav keeps 11 decimals of p, T, u and recomputes
+// rho and w on load, psstFiniteVolumeGrid.cpp:559-639, 279-300, so a restart
+// from it does not continue the run exactly.)
+struct CkptHeader {
+    char magic[8];
+    int32_t dim, precision;
+    int64_t nvol, nint, iter;
+};
+constexpr char kCkptMagic[8] = {'P', 'S', 'S', 'T', 'C', 'K', 'P', '1'};
+
+template <typename R>
+void save_checkpoint(psst_solver *s, const char *path) {
+    const int64_t nv = s->nvol_ref;
+    std::vector<double> prim((size_t)(2 + s->dim) * nv), w((size_t)s->nv * nv), rho(nv);
+    get_state<R>(s, prim.data(), w.data());
+    {
+        std::vector<CellRec<R>> h(s->L.nall);
+        ck(cudaMemcpyAsync(h.data(), states<R>(s)[s->cur].rec, h.size() * sizeof(CellRec<R>),
+                           cudaMemcpyDeviceToHost, s->stream),
+           "copy");
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+        for (int32_t d = 0; d < s->L.nall; ++d) rho[s->L.vol_of_dev[d]] = (double)h[d].v[RRHO];
+    }
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.dim = s->dim;
+    h.precision = s->sc.precision;
+    h.nvol = nv;
+    h.nint = s->L.nint;
+    h.iter = s->iter;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) raise(PSST_ERR_IO, std::string("cannot write ") + path);
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+              std::fwrite(prim.data(), sizeof(double), prim.size(), f) == prim.size() &&
+              std::fwrite(rho.data(), sizeof(double), rho.size(), f) == rho.size() &&
+              std::fwrite(w.data(), sizeof(double), w.size(), f) == w.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) raise(PSST_ERR_IO, std::string("cannot write ") + path);
+}
+
+template <typename R>
+void load_checkpoint(psst_solver *s, const char *path) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) raise(PSST_ERR_IO, std::string("cannot read ") + path);
+    CkptHeader h{};
+    const int64_t nv = s->nvol_ref;
+    std::vector<double> prim((size_t)(2 + s->dim) * nv), w((size_t)s->nv * nv), rho(nv);
+    bool ok = std::fread(&h, sizeof h, 1, f) == 1 && std::memcmp(h.magic, kCkptMagic, 8) == 0;
+    const bool match = ok && h.dim == s->dim && h.nvol == nv && h.nint == s->L.nint;
+    ok = match && h.precision == s->sc.precision &&
+         std::fread(prim.data(), sizeof(double), prim.size(), f) == prim.size() &&
+         std::fread(rho.data(), sizeof(double), rho.size(), f) == rho.size() &&
+         std::fread(w.data(), sizeof(double), w.size(), f) == w.size();
+    std::fclose(f);
+    if (!match) raise(PSST_ERR_FORMAT, std::string(path) + ": not a checkpoint of this grid");
+    if (!ok) raise(PSST_ERR_FORMAT, std::string(path) + ": truncated, or written at another precision");
+    ensure_staging(s);
+    ck(cudaMemcpyAsync(s->d_prim, prim.data(), prim.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "state upload");
+    ck(cudaMemcpyAsync(s->d_rho, rho.data(), rho.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "state upload");
+    ck(cudaMemcpyAsync(s->d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "state upload");
+    Ops<R>::set_exact(s->dim, s->g, states<R>(s)[s->cur], work<R>(s), s->d_prim, s->d_rho, s->d_w, s->d_vol, nv,
+                      s->stream);
+    ck(cudaGetLastError(), "checkpoint state");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    s->iter = h.iter;
 }
 
 template <typename R, int DIM>
@@ -1149,6 +1224,24 @@ extern "C" psst_status psst_solver_get_state(psst_solver *s, double *prim, doubl
     if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     DISPATCH(s, get_state)(s, prim, w);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_save_checkpoint(psst_solver *s, const char *path) {
+    PSST_API_BEGIN
+    if (!s || !path) raise(PSST_ERR_ARG, "psst_solver_save_checkpoint: null argument");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, save_checkpoint)(s, path);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_load_checkpoint(psst_solver *s, const char *path) {
+    PSST_API_BEGIN
+    if (!s || !path) raise(PSST_ERR_ARG, "psst_solver_load_checkpoint: null argument");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    DISPATCH(s, load_checkpoint)(s, path);
+    s->has_state = true;
     PSST_API_END
 }
 

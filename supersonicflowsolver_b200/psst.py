@@ -200,6 +200,14 @@ class Solver:
         check(_lib.load().psst_solver_get_state(self._h, _ptr(prim), _ptr(w) if with_w else None))
         return (prim, w) if with_w else prim
 
+    def save_checkpoint(self, path):
+        """Full-precision state + iteration counter (exact resume; see
+        psst_solver_save_checkpoint)."""
+        check(_lib.load().psst_solver_save_checkpoint(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path):
+        check(_lib.load().psst_solver_load_checkpoint(self._h, str(path).encode()))
+
     def gradient_calculate(self):
         check(_lib.load().psst_gradient_calculate(self._h))
 

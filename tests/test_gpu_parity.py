@@ -292,3 +292,35 @@ def test_nonfinite_state_reports_error(tmp_path):
     s.set_state(prim)
     linf, _ = s.explicit_solve(1)
     assert np.all(np.isfinite(linf))
+
+
+@pytest.mark.parametrize("precision,lc1_mode,mesh", [(64, 0, "j"), (32, 1, "t"), (64, 1, "a")],
+                         ids=["fp64_sequential_2d", "fp32_jacobi_3d", "fp64_jacobi_adapted"])
+def test_checkpoint_resumes_exactly(tmp_path, precision, lc1_mode, mesh):
+    """N iterations, checkpoint, a new solver loads it, M more iterations:
+    state, conservative state, residual columns and the iteration counter
+    equal those of N + M iterations in one solver, bit for bit (the .sav,
+    rounded to 11 decimals, cannot do this)."""
+    m = MESH[mesh]()
+    path, d, name = make_case(tmp_path, m, max_iter=9, flux=3, order=2, limiter=5 if m.dim == 3 else 4, lc=1,
+                              rk_level=4, mach=3.0 if m.dim == 3 else 2.5)
+    g, a = gpu_solver(path, d, name, precision=precision, lc1_mode=lc1_mode)
+    la, _ = a.explicit_solve(9)
+    _, b = gpu_solver(path, d, name, precision=precision, lc1_mode=lc1_mode)
+    b.explicit_solve(5)
+    ck = str(tmp_path / "state.ckpt")
+    b.save_checkpoint(ck)
+    _, c = gpu_solver(path, d, name, precision=precision, lc1_mode=lc1_mode)
+    c.load_checkpoint(ck)
+    assert c.iter == b.iter == 6
+    lc, _ = c.explicit_solve(4)
+    assert np.array_equal(lc, la[5:])
+    pa, wa = a.get_state(with_w=True)
+    pc, wc = c.get_state(with_w=True)
+    assert np.array_equal(pa, pc) and np.array_equal(wa, wc)
+    assert np.array_equal(a.get("rho"), c.get("rho"))
+    assert a.iter == c.iter
+    sc64 = 32 if precision == 64 else 64
+    _, e = gpu_solver(path, d, name, precision=sc64, lc1_mode=lc1_mode)
+    with pytest.raises(PsstError):
+        e.load_checkpoint(ck)
