@@ -412,6 +412,41 @@ def fp64_and_precision(args, grid, sc, prim, fp32_solver, stream_ptr, dev, n_pre
     return rec, {"iterations": n_prec, "fp32_vs_fp64": err}
 
 
+def gemm_throughput():
+    """The learned part's tensor-core GEMM (psst_tc_gemm_bf16, tcgen05 BF16 ->
+    FP32) on the warm-start network's training shapes: a hidden layer forward
+    (16384 points x 256 outputs x 256 inputs, both operands contiguous along
+    K) and its weight gradient (256 x 256 over 16384 points, both operands
+    contiguous along M/N, split over K in 256-row slices). TFLOP/s against
+    the measured BF16 peak and against each shape's own HBM bound (operands
+    read once, FP32 result written once)."""
+    import torch
+    from supersonicflowsolver_b200.mlp import tc_gemm_time
+
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    d = json.load(open(p)) if os.path.exists(p) else {}
+    peak, peak_kind = (d["bf16_tflops"], "measured") if "bf16_tflops" in d else (1590.0, "fallback")
+    hbm, _ = peaks()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn((16384, 256), generator=g, device="cuda").to(torch.bfloat16)
+    W = torch.randn((256, 256), generator=g, device="cuda").to(torch.bfloat16)
+    Y = torch.randn((16384, 256), generator=g, device="cuda").to(torch.bfloat16)
+    out = {"peak_tflops": peak, "peak_kind": peak_kind}
+    for name, kw, M, N, K, dbytes in (
+            ("forward_16384x256x256", dict(A=X, B=W), 16384, 256, 256, 16384 * 256 * 4),
+            ("weight_grad_256x256x16384", dict(A=X, B=Y, a_strides=(1, 256), b_strides=(1, 256), M=256, N=256,
+                                               K=16384, k_split=256), 256, 256, 16384, 64 * 256 * 256 * 4)):
+        tc_gemm_time(reps=3, **kw)
+        ms = tc_gemm_time(reps=20, **kw)
+        flops = 2.0 * M * N * K
+        byts = 2.0 * (M * K + N * K) + dbytes
+        tf = flops / (ms * 1e-3) / 1e12
+        bound = min(peak, flops / (byts / (hbm * 1e9)) / 1e12)
+        out[name] = {"ms": ms, "tflops": tf, "frac_of_peak": tf / peak, "hbm_bound_tflops": bound,
+                     "frac_of_shape_bound": tf / bound}
+    return out
+
+
 def run_gpu(args):
     import torch
 
@@ -517,6 +552,8 @@ def run_gpu(args):
     extra = {}
     if args.workload == "wedge3d_6M_tets" and not args.no_fp64 and ws == 1:
         extra["fp64"], extra["precision"] = fp64_and_precision(args, grid, sc, prim, solver, stream.cuda_stream, dev)
+    if args.workload == "wedge3d_6M_tets" and ws == 1:
+        extra["tensor_gemm"] = gemm_throughput()
     if rank == 0:
         nv = grid.dim + 2
         state_bytes = (2 + grid.dim) * grid.nvol * 8

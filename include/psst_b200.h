@@ -434,9 +434,29 @@ void psst_mlp_destroy(psst_mlp *m);
  * A[m][k] * B[n][k], BF16 device operands given by element strides
  * (A[m][k] = A[m*a_sm + k*a_sk], B[n][k] = B[n*b_sn + k*b_sk]), FP32 device
  * output with row stride d_sm, z over ceil(K / k_split) splits (plain element
- * sum of the splits = the full product). Synchronises the stream. */
+ * sum of the splits = the full product). Synchronises the stream. Operands
+ * contiguous along K (a_sk or b_sk == 1) or along M/N (a_sm or b_sn == 1, the
+ * other stride a multiple of 8) load as 16-byte vectors; other strides
+ * element by element. */
 psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn, int64_t b_sk,
                               int M, int N, int K, int k_split, float *D, int64_t d_sm, void *stream);
+
+/* psst_tc_gemm_bf16 launched reps times back to back between two CUDA events
+ * on `stream`; *ms receives the mean device time of one launch (the GEMM's
+ * throughput without the per-call synchronisation). */
+psst_status psst_tc_gemm_bf16_time(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
+                                   int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
+                                   void *stream, int reps, double *ms);
+
+/* psst_tc_gemm_bf16 with the bound of its first mbarrier wait that runs out
+ * given in polls (< 0: the default, about a second; 0: that wait gives up at
+ * once). A wait that runs out makes the call return PSST_ERR_TIMEOUT after a
+ * second, full-length wait for the tensor-core work in flight, so no MMA is
+ * running when the kernel frees its tensor memory; D is then undefined. Used
+ * to test the timeout path without stalling a GPU. */
+psst_status psst_tc_gemm_bf16_wait(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
+                                   int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
+                                   void *stream, int64_t wait_polls);
 
 #ifdef __cplusplus
 }

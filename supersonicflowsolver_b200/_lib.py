@@ -33,6 +33,7 @@ EXPORTED = [
     "psst_solver_load_checkpoint",
     "psst_mlp_create", "psst_mlp_param_count", "psst_mlp_get_params", "psst_mlp_set_params", "psst_mlp_forward",
     "psst_mlp_gradients", "psst_mlp_train_step", "psst_mlp_set_stream", "psst_mlp_destroy", "psst_tc_gemm_bf16",
+    "psst_tc_gemm_bf16_wait", "psst_tc_gemm_bf16_time",
 ]
 
 
@@ -141,6 +142,8 @@ def load():
         "psst_mlp_set_stream": (I, [P, P]),
         "psst_mlp_destroy": (None, [P]),
         "psst_tc_gemm_bf16": (I, [P, I64, I64, P, I64, I64, I, I, I, I, P, I64, P]),
+        "psst_tc_gemm_bf16_wait": (I, [P, I64, I64, P, I64, I64, I, I, I, I, P, I64, P, I64]),
+        "psst_tc_gemm_bf16_time": (I, [P, I64, I64, P, I64, I64, I, I, I, I, P, I64, P, I, ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

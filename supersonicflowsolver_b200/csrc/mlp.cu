@@ -12,13 +12,19 @@
 //
 // GEMM kernel: one CTA computes a 128 x NT tile of D = A . B^T, A [M x K],
 // B [N x K] given by element strides (so transposed operands need no copy).
-// Each 64-wide K chunk is staged in shared memory in the UMMA K-major
-// no-swizzle layout (8-row x 16-byte core matrices), issued as four
-// tcgen05.mma.kind::f16 (M = 128, N = NT, K = 16) by one thread, committed to
-// an mbarrier that the CTA waits on (bounded) before reusing the buffers;
-// the epilogue reads the accumulator with tcgen05.ld (one row per thread) and
-// applies bias / SiLU / SiLU-derivative. Split-K over gridDim.z writes FP32
-// partials that a second kernel sums in a fixed order (deterministic).
+// K is walked in 64-wide chunks through two shared-memory stages in the UMMA
+// K-major no-swizzle layout (8-row x 16-byte core matrices): while the tensor
+// core runs the four tcgen05.mma.kind::f16 (M = 128, N = NT, K = 16) of chunk
+// k, issued by one thread and committed to that stage's mbarrier, the CTA
+// stages chunk k+1 into the other stage. Operands contiguous along K load as
+// 16-byte vectors; operands contiguous along M/N (the transposed ones) load as
+// 16-byte vectors along M/N and are transposed in registers, 8 x 8 at a time.
+// The epilogue reads the accumulator with tcgen05.ld (one row per thread),
+// applies bias / SiLU / SiLU-derivative, and writes through a per-warp
+// shared-memory tile so that global stores are row-contiguous. Split-K over
+// gridDim.z writes FP32 partials that a second kernel sums in a fixed order
+// (deterministic). Every mbarrier wait is bounded.
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -38,6 +44,7 @@ constexpr int kTileM = 128;
 constexpr int kChunkK = 64;
 constexpr int kThreads = 128;
 constexpr unsigned kWaitLimit = 1u << 26;  // mbarrier polls before giving up (~seconds)
+constexpr int kStages = 2;                 // operand stages in shared memory
 
 enum Epi { EPI_NONE = 0, EPI_SILU = 1, EPI_DSILU = 2 };
 enum MlpErr { MLP_ERR_TIMEOUT = 1 };
@@ -62,10 +69,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// Polls the mbarrier phase with a bound; false if it never completed.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+// Polls the mbarrier phase at most `limit` times; false if it never completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, unsigned limit = kWaitLimit) {
     const uint32_t a = smem_u32(bar);
-    for (unsigned i = 0; i < kWaitLimit; ++i) {
+    for (unsigned i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -130,11 +137,17 @@ struct GemmArgs {
     bf16 *Z16;           // BF16 pre-activation output [M][d_sm] (EPI_SILU, or null)
     int64_t d_sm;
     int *err;
+    unsigned wait_polls;  // bound of the first wait that runs out (kWaitLimit; 0 gives up at once)
 };
 
-// Stages rows [r0, r0+rows) x K columns [k0, k0+64) of a strided BF16 matrix
-// into the K-major no-swizzle layout: element (r, k) at
-// ((k/8) * rows + r) * 16 + (k%8) * 2 bytes. Out-of-range elements are zero.
+// Stages rows [r0, r0+ROWS) x K columns [k0, k0+64) of a strided BF16 matrix
+// (element (r, k) at g[r * sr + k * sk]) into the K-major no-swizzle layout:
+// element (r, k) at ((k/8) * ROWS + r) * 16 + (k%8) * 2 bytes. Out-of-range
+// elements (r >= nrows, k >= kend) are zero.
+//  * contiguous along K (sk == 1): one 16-byte load per (row, 8 k);
+//  * contiguous along the rows (sr == 1): one 16-byte load per (8 rows, k),
+//    eight of them (8 k) transposed in registers into eight (row, 8 k) units;
+//  * otherwise element by element.
 template <int ROWS>
 __device__ __forceinline__ void stage(bf16 *s, const bf16 *g, int64_t sr, int64_t sk, int r0, int nrows, int k0,
                                       int kend) {
@@ -156,6 +169,40 @@ __device__ __forceinline__ void stage(bf16 *s, const bf16 *g, int64_t sr, int64_
             }
             *reinterpret_cast<int4 *>(s + ((size_t)kc * ROWS + r) * 8) = v;
         }
+    } else if (sr == 1 && (sk % 8) == 0 && ((uintptr_t)g & 15) == 0) {
+        for (int i = threadIdx.x; i < ROWS; i += kThreads) {  // (8-row block, 8-k group) per i
+            const int rb = (i % (ROWS / 8)) * 8, kc = i / (ROWS / 8);
+            uint32_t v[8][4];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int k = k0 + kc * 8 + j;
+                int4 t = make_int4(0, 0, 0, 0);
+                if (k < kend) {
+                    const bf16 *src = g + (int64_t)k * sk + r0 + rb;
+                    if (r0 + rb + 8 <= nrows) {
+                        t = *reinterpret_cast<const int4 *>(src);
+                    } else {
+                        bf16 e[8];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) e[q] = r0 + rb + q < nrows ? src[q] : __float2bfloat16(0.0f);
+                        memcpy(&t, e, 16);
+                    }
+                }
+                v[j][0] = (uint32_t)t.x, v[j][1] = (uint32_t)t.y, v[j][2] = (uint32_t)t.z, v[j][3] = (uint32_t)t.w;
+            }
+            // v[j] holds rows rb..rb+7 of column j (two rows per word); row r of
+            // the unit takes the half r%2 of word r/2 from columns 2q, 2q+1
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint32_t sel = (r & 1) ? 0x7632u : 0x5410u;
+                int4 o;
+                o.x = (int)__byte_perm(v[0][r >> 1], v[1][r >> 1], sel);
+                o.y = (int)__byte_perm(v[2][r >> 1], v[3][r >> 1], sel);
+                o.z = (int)__byte_perm(v[4][r >> 1], v[5][r >> 1], sel);
+                o.w = (int)__byte_perm(v[6][r >> 1], v[7][r >> 1], sel);
+                *reinterpret_cast<int4 *>(s + ((size_t)kc * ROWS + rb + r) * 8) = o;
+            }
+        }
     } else {
         for (int i = threadIdx.x; i < ROWS * kChunkK; i += kThreads) {
             const int r = i % ROWS, kk = i / ROWS;
@@ -168,23 +215,22 @@ __device__ __forceinline__ void stage(bf16 *s, const bf16 *g, int64_t sr, int64_
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kThreads, 1) k_gemm(GemmArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_gemm(GemmArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    bf16 *sA = reinterpret_cast<bf16 *>(smem);                       // 128 x 64
-    bf16 *sB = reinterpret_cast<bf16 *>(smem + kTileM * kChunkK * 2);  // NT x 64
-    __shared__ __align__(8) uint64_t bar;
+    constexpr int kStageBytes = (kTileM + NT) * kChunkK * 2;
+    __shared__ __align__(8) uint64_t bar[kStages];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
     const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * NT;
     const int kb = blockIdx.z * a.k_split, ke = min(a.K, kb + a.k_split);
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                      "r"(NT < 32 ? 32 : NT));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
+        for (int b = 0; b < kStages; ++b) mbar_init(&bar[b], 1);
         failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -192,9 +238,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(GemmArgs a) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
-    unsigned phase = 0;
-    int nchunks = 0;
-    for (int k0 = kb; k0 < ke; k0 += kChunkK, ++nchunks) {
+    unsigned phase = 0u;  // bit b: the phase of stage b's mbarrier to wait for
+    unsigned polls = a.wait_polls;  // the first wait that runs out uses this bound, the drain kWaitLimit
+    // thread 0: waits (bounded) for the MMAs committed to stage b; on a wait
+    // that runs out it marks the launch failed and waits (bounded again) for
+    // the latest commit, stage `newest`, which covers every MMA issued, so no
+    // MMA is in flight when the accumulator is freed
+    auto wait_stage = [&](int b, int newest) {
+        if (threadIdx.x == 0 && !failed) {
+            if (polls == 0 || !mbar_wait(&bar[b], (phase >> b) & 1u, polls)) {
+                failed = 1;
+                mbar_wait(&bar[newest], (phase >> newest) & 1u);
+            }
+        }
+        phase ^= 1u << b;
+    };
+    const int nchunks = ke > kb ? (ke - kb + kChunkK - 1) / kChunkK : 0;
+    for (int c = 0; c < nchunks; ++c) {
+        const int b = c % kStages;
+        if (c >= kStages) wait_stage(b, (c - 1) % kStages);  // the MMAs of chunk c - 2 read this stage
+        __syncthreads();
+        if (failed) break;
+        bf16 *sA = reinterpret_cast<bf16 *>(smem + b * kStageBytes);
+        bf16 *sB = reinterpret_cast<bf16 *>(smem + b * kStageBytes + kTileM * kChunkK * 2);
+        const int k0 = kb + c * kChunkK;
         stage<kTileM>(sA, a.A, a.a_sm, a.a_sk, m0, a.M, k0, ke);
         stage<NT>(sB, a.B, a.b_sn, a.b_sk, n0, a.N, k0, ke);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -203,56 +270,69 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(GemmArgs a) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t abase = smem_u32(sA), bbase = smem_u32(sB);
 #pragma unroll
-            for (int s = 0; s < kChunkK / 16; ++s) {
-                const uint64_t da = umma_desc(abase + 2 * s * kTileM * 16, kTileM * 16, 128);
-                const uint64_t db = umma_desc(bbase + 2 * s * NT * 16, NT * 16, 128);
-                umma_bf16<NT>(tmem, da, db, (nchunks > 0 || s > 0) ? 1u : 0u);
+            for (int q = 0; q < kChunkK / 16; ++q) {
+                const uint64_t da = umma_desc(abase + 2 * q * kTileM * 16, kTileM * 16, 128);
+                const uint64_t db = umma_desc(bbase + 2 * q * NT * 16, NT * 16, 128);
+                umma_bf16<NT>(tmem, da, db, (c > 0 || q > 0) ? 1u : 0u);
             }
-            umma_commit(&bar);
-            // one thread waits (bounded) so the decision to go on is uniform
-            if (!mbar_wait(&bar, phase)) {
-                failed = 1;
-                mbar_wait(&bar, phase);  // second bounded wait for the MMAs in flight
-            }
+            umma_commit(&bar[b]);
         }
-        phase ^= 1;
-        __syncthreads();
-        if (failed) break;
     }
+    // the last commit covers every MMA issued before it
+    if (nchunks > 0 && !failed) wait_stage((nchunks - 1) % kStages, (nchunks - 1) % kStages);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (failed) {
         if (threadIdx.x == 0) atomicExch(a.err, MLP_ERR_TIMEOUT);
     } else {
-        // epilogue: thread t owns row m0 + t (TMEM lane t of this warp's quarter)
-        const int row = threadIdx.x;
-        const int m = m0 + row;
+        // epilogue: thread t holds row m0 + t (TMEM lane t); each warp writes its
+        // 32 rows x 32 columns at a time through its own shared tile, a row per
+        // store instruction (the operand stages are free now)
+        float *tf = reinterpret_cast<float *>(smem) + warp * 32 * 33;
+        bf16 *th = reinterpret_cast<bf16 *>(smem + 4 * 32 * 33 * 4) + warp * 32 * 34;
+        bf16 *tz = reinterpret_cast<bf16 *>(smem + 4 * 32 * 33 * 4 + 4 * 32 * 34 * 2) + warp * 32 * 34;
+        const int rw = warp * 32;  // first row of this warp in the tile
         const bool empty = nchunks == 0;
-        for (int c0 = 0; c0 < NT; c0 += 32) {
+        for (int c0 = 0; c0 < NT && n0 + c0 < a.N; c0 += 32) {
             float v[32];
             if (!empty)
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+                tmem_ld32(tmem + ((uint32_t)rw << 16) + (uint32_t)c0, v);
             else
 #pragma unroll
                 for (int i = 0; i < 32; ++i) v[i] = 0.0f;
-            if (m >= a.M) continue;
-#pragma unroll 4
+            const int nn = n0 + c0 + lane;  // column this lane stores
+            if (a.epi == EPI_DSILU) {        // the pre-activations of these rows, loaded row by row
+                for (int r = 0; r < 32; ++r) {
+                    const int m = m0 + rw + r;
+                    if (m < a.M && nn < a.N) tz[r * 34 + lane] = a.Zin[(int64_t)m * a.d_sm + nn];
+                }
+                __syncwarp();
+            }
+#pragma unroll
             for (int i = 0; i < 32; ++i) {
                 const int n = n0 + c0 + i;
-                if (n >= a.N) break;
                 float z = v[i];
-                if (a.bias) z += a.bias[n];
-                const int64_t o = (int64_t)m * a.d_sm + n;
-                if (a.D32) a.D32[(int64_t)blockIdx.z * a.M * a.d_sm + o] = z;
+                if (a.bias && n < a.N) z += a.bias[n];
+                tf[lane * 33 + i] = z;
                 if (a.epi == EPI_SILU) {
-                    if (a.Z16) a.Z16[o] = __float2bfloat16(z);
-                    if (a.D16) a.D16[o] = __float2bfloat16(silu(z));
+                    th[lane * 34 + i] = __float2bfloat16(silu(z));
                 } else if (a.epi == EPI_DSILU) {
-                    if (a.D16) a.D16[o] = __float2bfloat16(z * dsilu(__bfloat162float(a.Zin[o])));
-                } else if (a.D16) {
-                    a.D16[o] = __float2bfloat16(z);
+                    th[lane * 34 + i] = __float2bfloat16(z * dsilu(__bfloat162float(tz[lane * 34 + i])));
+                } else {
+                    th[lane * 34 + i] = __float2bfloat16(z);
                 }
             }
+            __syncwarp();
+            for (int r = 0; r < 32; ++r) {
+                const int m = m0 + rw + r;
+                if (m >= a.M || nn >= a.N) continue;
+                const int64_t o = (int64_t)m * a.d_sm + nn;
+                const float z = tf[r * 33 + lane];
+                if (a.D32) a.D32[(int64_t)blockIdx.z * a.M * a.d_sm + o] = z;
+                if (a.epi == EPI_SILU && a.Z16) a.Z16[o] = __float2bfloat16(z);
+                if (a.D16) a.D16[o] = th[r * 34 + lane];
+            }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -279,7 +359,7 @@ constexpr int kFeat = 128;       // Fourier features, padded
 constexpr int kFreq = 15;
 constexpr int kIn = 4, kOut = 4;
 constexpr int kHidden = 5;       // layers with SiLU
-constexpr int kSplitRows = 2048; // batch rows per split of a weight-gradient GEMM
+constexpr int kSplitRows = 256;  // batch rows per split of a weight-gradient GEMM (16384 rows: 128 CTAs)
 
 // Fourier features of x[b][4] (inputs normalised to [-1, 1]).
 __global__ void k_features(const float *x, int B, bf16 *f) {
@@ -456,6 +536,7 @@ GemmArgs gargs(const bf16 *A, int64_t a_sm, int64_t a_sk, const bf16 *B, int64_t
     a.K = K;
     a.k_split = K;
     a.err = err;
+    a.wait_polls = kWaitLimit;
     return a;
 }
 
@@ -714,11 +795,13 @@ extern "C" psst_status psst_mlp_set_stream(psst_mlp *m, void *stream) {
 
 extern "C" void psst_mlp_destroy(psst_mlp *m) { delete m; }
 
-// D[z][m][n] = sum over k in split z of A[m][k] B[n][k] (BF16 in, FP32 out).
-extern "C" psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
-                                         int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
-                                         void *stream) {
-    MLP_BEGIN
+namespace {
+
+// reps > 1 (timing): the kernel launched reps times back to back between two
+// events; *ms receives the mean device time of one launch.
+void tc_gemm(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn, int64_t b_sk, int M, int N,
+             int K, int k_split, float *D, int64_t d_sm, void *stream, unsigned wait_polls, int reps = 1,
+             double *ms = nullptr) {
     if (!A || !B || !D || M <= 0 || N <= 0 || K < 0 || k_split <= 0 || d_sm < N)
         raise(PSST_ERR_ARG, "psst_tc_gemm_bf16: bad argument");
     static thread_local int *err = nullptr;
@@ -735,12 +818,30 @@ extern "C" psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_
     a.k_split = k_split;
     a.D32 = D;
     a.d_sm = d_sm;
+    a.wait_polls = wait_polls;
     const int splits = K == 0 ? 1 : (K + k_split - 1) / k_split;
-    if (N <= 128)
-        gemm<128>(a, splits, s);
-    else
-        gemm<256>(a, splits, s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        ck(cudaEventRecord(e0, s), "event");
+    }
+    for (int r = 0; r < std::max(reps, 1); ++r) {
+        if (N <= 128)
+            gemm<128>(a, splits, s);
+        else
+            gemm<256>(a, splits, s);
+    }
     ck(cudaGetLastError(), "gemm launch");
+    if (ms) {
+        ck(cudaEventRecord(e1, s), "event");
+        ck(cudaEventSynchronize(e1), "event");
+        float t = 0.0f;
+        ck(cudaEventElapsedTime(&t, e0, e1), "event");
+        *ms = t / std::max(reps, 1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     int e = 0;
     ck(cudaMemcpyAsync(&e, err, sizeof e, cudaMemcpyDeviceToHost, s), "error word");
     ck(cudaStreamSynchronize(s), "stream sync");
@@ -748,5 +849,35 @@ extern "C" psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_
         cudaMemset(err, 0, sizeof(int));
         raise(PSST_ERR_TIMEOUT, "tensor-core GEMM: an mbarrier wait ran out");
     }
+}
+
+}  // namespace
+
+// D[z][m][n] = sum over k in split z of A[m][k] B[n][k] (BF16 in, FP32 out).
+extern "C" psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
+                                         int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
+                                         void *stream) {
+    MLP_BEGIN
+    tc_gemm(A, a_sm, a_sk, B, b_sn, b_sk, M, N, K, k_split, D, d_sm, stream, kWaitLimit);
+    MLP_END
+}
+
+// Device time of one launch, the mean over reps back-to-back launches.
+extern "C" psst_status psst_tc_gemm_bf16_time(const void *A, int64_t a_sm, int64_t a_sk, const void *B,
+                                              int64_t b_sn, int64_t b_sk, int M, int N, int K, int k_split,
+                                              float *D, int64_t d_sm, void *stream, int reps, double *ms) {
+    MLP_BEGIN
+    if (reps <= 0 || !ms) raise(PSST_ERR_ARG, "psst_tc_gemm_bf16_time: reps > 0 and ms needed");
+    tc_gemm(A, a_sm, a_sk, B, b_sn, b_sk, M, N, K, k_split, D, d_sm, stream, kWaitLimit, reps, ms);
+    MLP_END
+}
+
+// The same with the bound of the first mbarrier wait given (in polls).
+extern "C" psst_status psst_tc_gemm_bf16_wait(const void *A, int64_t a_sm, int64_t a_sk, const void *B,
+                                              int64_t b_sn, int64_t b_sk, int M, int N, int K, int k_split,
+                                              float *D, int64_t d_sm, void *stream, int64_t wait_polls) {
+    MLP_BEGIN
+    tc_gemm(A, a_sm, a_sk, B, b_sn, b_sk, M, N, K, k_split, D, d_sm, stream,
+            wait_polls < 0 || wait_polls > (int64_t)kWaitLimit ? kWaitLimit : (unsigned)wait_polls);
     MLP_END
 }

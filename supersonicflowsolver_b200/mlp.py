@@ -109,9 +109,11 @@ class MLP:
             pass
 
 
-def tc_gemm(A, B, k_split=None, a_strides=None, b_strides=None, M=None, N=None, K=None):
+def tc_gemm(A, B, k_split=None, a_strides=None, b_strides=None, M=None, N=None, K=None, wait_polls=None, out=None):
     """D = A . B^T on the tensor cores. A [M][K], B [N][K] torch CUDA BF16 (or
-    any strides given explicitly); returns FP32 [splits][M][N] partials."""
+    any strides given explicitly); returns FP32 [splits][M][N] partials.
+    wait_polls: bound of the first mbarrier wait (psst_tc_gemm_bf16_wait);
+    out: a preallocated [splits][M][N] FP32 result."""
     import torch
 
     M = M if M is not None else A.shape[0]
@@ -121,7 +123,32 @@ def tc_gemm(A, B, k_split=None, a_strides=None, b_strides=None, M=None, N=None, 
     b_sn, b_sk = b_strides if b_strides else B.stride()
     k_split = k_split or max(K, 1)
     splits = max(1, -(-K // k_split))
-    D = torch.zeros((splits, M, N), dtype=torch.float32, device=A.device)
-    check(_lib.load().psst_tc_gemm_bf16(A.data_ptr(), a_sm, a_sk, B.data_ptr(), b_sn, b_sk, M, N, K, k_split,
-                                         D.data_ptr(), N, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    D = out if out is not None else torch.zeros((splits, M, N), dtype=torch.float32, device=A.device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if wait_polls is None:
+        check(_lib.load().psst_tc_gemm_bf16(A.data_ptr(), a_sm, a_sk, B.data_ptr(), b_sn, b_sk, M, N, K, k_split,
+                                             D.data_ptr(), N, stream))
+    else:
+        check(_lib.load().psst_tc_gemm_bf16_wait(A.data_ptr(), a_sm, a_sk, B.data_ptr(), b_sn, b_sk, M, N, K,
+                                                  k_split, D.data_ptr(), N, stream, int(wait_polls)))
     return D
+
+
+def tc_gemm_time(A, B, reps=20, k_split=None, a_strides=None, b_strides=None, M=None, N=None, K=None):
+    """Mean device milliseconds of one tensor-core GEMM launch (reps launches
+    back to back between CUDA events); same operands as tc_gemm."""
+    import torch
+
+    M = M if M is not None else A.shape[0]
+    K = K if K is not None else A.shape[1]
+    N = N if N is not None else B.shape[0]
+    a_sm, a_sk = a_strides if a_strides else A.stride()
+    b_sn, b_sk = b_strides if b_strides else B.stride()
+    k_split = k_split or max(K, 1)
+    splits = max(1, -(-K // k_split))
+    D = torch.empty((splits, M, N), dtype=torch.float32, device=A.device)
+    ms = ctypes.c_double()
+    check(_lib.load().psst_tc_gemm_bf16_time(A.data_ptr(), a_sm, a_sk, B.data_ptr(), b_sn, b_sk, M, N, K, k_split,
+                                              D.data_ptr(), N, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                              int(reps), ctypes.byref(ms)))
+    return ms.value

@@ -93,3 +93,39 @@ def test_mlp_training_reduces_loss():
     for _ in range(301):
         net2.train_step(xd, td, 1e-3)
     assert np.array_equal(net.params(), net2.params())
+
+
+@pytest.mark.parametrize("M,N,K", [(200, 72, 1000), (256, 256, 4096), (40, 136, 64)])
+def test_tc_gemm_transposed_ragged(M, N, K):
+    """Operands contiguous along M and N (the weight-gradient form), with row
+    counts that are not multiples of the 8-row load units and a ragged last
+    K chunk: loaded as 16-byte vectors and transposed in registers."""
+    from supersonicflowsolver_b200.mlp import tc_gemm
+
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    X = torch.randn((K, M), generator=g, device="cuda").to(torch.bfloat16)  # [batch][M]
+    Y = torch.randn((K, N), generator=g, device="cuda").to(torch.bfloat16)  # [batch][N]
+    D = tc_gemm(X, Y, k_split=512, a_strides=(1, M), b_strides=(1, N), M=M, N=N, K=K).sum(dim=0)
+    ref = X.float().T @ Y.float()
+    bound = (X.float().abs().T @ Y.float().abs()) * (K * 2.0 ** -23) + 1e-6
+    assert torch.all((D - ref).abs() <= bound), float(((D - ref).abs() / bound).max())
+
+
+def test_tc_gemm_wait_that_runs_out_is_reported():
+    """A first mbarrier wait bounded at zero polls gives up at once: the call
+    returns PSST_ERR_TIMEOUT (after draining the MMAs in flight), and the next
+    call with the default bound computes the product."""
+    from supersonicflowsolver_b200.mlp import tc_gemm
+    from supersonicflowsolver_b200.psst import PsstError
+
+    g = torch.Generator(device="cuda").manual_seed(11)
+    A = torch.randn((256, 512), generator=g, device="cuda").to(torch.bfloat16)
+    B = torch.randn((256, 512), generator=g, device="cuda").to(torch.bfloat16)
+    for polls in (0, 0):
+        with pytest.raises(PsstError) as e:
+            tc_gemm(A, B, wait_polls=polls)
+        assert e.value.status == 7
+    D = tc_gemm(A, B, wait_polls=-1)[0]
+    ref = A.float() @ B.float().T
+    bound = (A.float().abs() @ B.float().abs().T) * (512 * 2.0 ** -23) + 1e-6
+    assert torch.all((D - ref).abs() <= bound)
