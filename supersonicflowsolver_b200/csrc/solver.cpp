@@ -469,6 +469,15 @@ struct psst_solver {
         allocs.push_back(p);
         return p;
     }
+    // frees a buffer from dalloc (null: nothing)
+    void dfree(void *p) {
+        if (!p) return;
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) {
+            allocs.erase(it);
+            cudaFree(p);
+        }
+    }
     template <class T>
     T *dalloc(size_t n) {
         return (T *)dalloc_bytes(std::max<size_t>(n, 1) * sizeof(T));
@@ -559,6 +568,10 @@ void reserve_norms(psst_solver *s, int n_iter) {
     DevWork<R> &w = work<R>(s);
     if (n_iter > s->norm_cap) {
         s->drop_graphs();
+        ck(cudaStreamSynchronize(s->stream), "stream sync");  // no launch still reads the old buffers
+        s->dfree(w.linf);
+        s->dfree(w.l2);
+        s->dfree(w.case_linf);
         s->norm_cap = std::max(n_iter, 2 * s->norm_cap);
         w.linf = s->dalloc<double>((size_t)s->norm_cap * s->nv);
         w.l2 = s->dalloc<double>((size_t)s->norm_cap * s->nv);
