@@ -343,7 +343,7 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         L.lvl_cells[fillp[level[d]]++] = d;
     }
     // wavefront schedule: period P = 1 + the largest level difference across
-    // an interior face; items of at most kWfBlock cells of one level (device
+    // an interior face; items of at most kWfBlock / kWfLanes cells of one level (device
     // order inside a level), ordered by level mod P, then level
     if (sc.lc == 1 && sc.lc1_mode == PSST_LC1_SEQUENTIAL && L.nint > 0) {
         int32_t D = 0;
@@ -363,10 +363,11 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
             const int32_t first = (int32_t)L.wf_item_level.size();
             for (int32_t l = r; l < L.nlevels; l += L.wf_period) {
                 L.wf_lvl_items[2 * (size_t)l] = (int32_t)L.wf_item_level.size();
-                for (int32_t b = L.lvl_ptr[l]; b < L.lvl_ptr[l + 1]; b += kWfBlock) {
+                const int32_t per_item = kWfBlock / kWfLanes;
+                for (int32_t b = L.lvl_ptr[l]; b < L.lvl_ptr[l + 1]; b += per_item) {
                     L.wf_item_ptr.push_back((int32_t)L.wf_cells.size());
                     L.wf_item_level.push_back(l);
-                    for (int32_t i = b; i < std::min(b + kWfBlock, L.lvl_ptr[l + 1]); ++i)
+                    for (int32_t i = b; i < std::min(b + per_item, L.lvl_ptr[l + 1]); ++i)
                         L.wf_cells.push_back(by_level[i]);
                 }
                 L.wf_lvl_items[2 * (size_t)l + 1] = (int32_t)L.wf_item_level.size();

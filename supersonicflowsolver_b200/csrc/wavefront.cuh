@@ -26,6 +26,16 @@
 #include "kernels.cuh"
 #include "ops.hpp"
 
+// CTAs per SM the wavefront kernel is built for (register cap 65536 / (128 x
+// this)): more co-resident CTAs take more of a step's work items at once. 2D:
+// three without spills; 3D: two (three would spill).
+#ifndef PSST_WF_MINB_2D
+#define PSST_WF_MINB_2D 3
+#endif
+#ifndef PSST_WF_MINB_3D
+#define PSST_WF_MINB_3D 2
+#endif
+
 namespace psst {
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
@@ -127,63 +137,115 @@ __device__ __forceinline__ void wf_gradient(const WfArgs<R> &a, int64_t k, int32
     }
 }
 
-// RK stage s (stage `stage` of iteration k) for cell c: the fluxes of its
-// faces in the reference's face-loop order (psstConvectiveFlow.cpp:289-299 as
-// a per-cell sum), the time step with the neighbours updated earlier in the
-// reference's order taken from this stage's output
-// (psstLocalTimeCalculation.cpp:90-131), the RK update and primitives
-// (psstFiniteVolumeGrid.cpp:324-346), and the cell's ghosts (:351-366).
+// RK stage s (stage `stage` of iteration k) for cell c, by the four lanes of a
+// quad (kWfLanes): lane q takes the cell's faces q, q+4, .. in the reference's
+// face-loop order for the fluxes (psstConvectiveFlow.cpp:289-299 as a per-cell
+// sum) and the faces q, q+4, .. of the cell's own order for the local time
+// step's neighbour terms (psstLocalTimeCalculation.cpp:90-131, neighbours
+// updated earlier in the reference's order read from this stage's output);
+// the quad then forms the residual sum and the time step's running sums face
+// by face in the reference's order through shuffles (every lane the same
+// values, in the same order, so the bits are the single-thread ones). Lane 0
+// does the RK update and primitives (psstFiniteVolumeGrid.cpp:324-346) and
+// the cell's ghosts (:351-366). qbase: the quad's first lane in the warp.
 template <typename R, int DIM, int REC, int LIM>
-__device__ __forceinline__ void wf_stage_cell(const WfArgs<R> &a, int64_t s, int64_t k, int stage, int32_t c,
-                                              double sq[DIM + 2], double mx[DIM + 2]) {
+__device__ __forceinline__ void wf_stage_quad(const WfArgs<R> &a, int64_t s, int64_t k, int stage, int32_t c, int q,
+                                              int qbase, double sq[DIM + 2], double mx[DIM + 2]) {
     constexpr int NV = DIM + 2;
+    const unsigned qmask = 0xFu << qbase;
     const DevGrid &g = a.g;
     const CellRec<R> *in = a.buf[(a.in_buf + s) & 1];
     CellRec<R> *out = a.buf[(a.in_buf + s + 1) & 1];
     const GradRec<R, DIM> *gr = reinterpret_cast<const GradRec<R, DIM> *>(a.gbuf[(a.n_iter - 1 - k) & 1]);
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     const int first = stage == 0;
-    const RkIn<NV> rin = rk_load_cg<R, NV>(g, a.wk, first, c);
+    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    const uint64_t perm = g.wperm[c];
+    const int32_t myrank = g.rank[c];
+    const Prim<R, DIM> own = unpack<R, DIM>(ldcg(in + c));
+    const R grm = (R)a.gas.gamma * (R)a.gas.rm;
+    const R cc = sqrt(grm * own.T);
     R res[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) res[v] = (R)0;
-    const int32_t b = g.csr_ptr[c], e = g.csr_ptr[c + 1];
-    for (int32_t q = b; q < e; ++q) {
-        const int32_t ent = g.csr_ent[q], f = ent >> 1;
-        const FaceRec<R, DIM> fr = ldg(frec + f);
-        R nn[DIM];
+    R den = (R)0, nnb = (R)0;
+    for (int r0 = 0; r0 < K; r0 += kWfLanes) {
+        const int j = r0 + q;
+        int32_t ent = 0;
+        R o[NV], pu[DIM], nvj = (R)0, cnj = (R)0, sj = (R)0;
+        if (j < K) {
+            // flux of the j-th face in face-loop order (the face pass's output value)
+            ent = g.csr_ent[b + j];
+            const int32_t f = ent >> 1;
+            const FaceRec<R, DIM> fr = ldg(frec + f);
+            // own-order position j: its neighbour for the time step
+            const int32_t ent2 = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
+            const FaceRec<R, DIM> fr2 = ent2 == ent ? fr : ldg(frec + (ent2 >> 1));
+            const int32_t nb = (ent2 & 1) ? fr2.c0 : fr2.c1;
+            const CellRec<R> *src = (nb < g.nint && g.rank[nb] < myrank) ? out : in;
+            const Prim<R, DIM> on = unpack<R, DIM>(ldcg(src + nb));
+            R nn[DIM];
 #pragma unroll
-        for (int k2 = 0; k2 < DIM; ++k2) nn[k2] = (R)fr.n[k2];
-        const Prim<R, DIM> p0 = unpack<R, DIM>(ldcg(in + fr.c0));
-        const Prim<R, DIM> p1 = unpack<R, DIM>(ldcg(in + fr.c1));
-        R flow[NV];
-        if (f < g.nfi) {
-            GradRec<R, DIM> g0, g1;
-            if (REC) {
-                g0 = ldcg(gr + fr.c0);
-                g1 = ldcg(gr + fr.c1);
-            }
-            Prim<R, DIM> r[2] = {p0, p1};
-            if (!wf_interior_flux<R, DIM, REC, LIM>(a.flux, r, &g0, &g1, fr, nn, a.gas, flow)) {
-                flag_error(a.wk.err, a.flux == 2 ? ERR_HLL : ERR_HLLC, f);
+            for (int k2 = 0; k2 < DIM; ++k2) nn[k2] = (R)fr.n[k2];
+            const Prim<R, DIM> p0 = unpack<R, DIM>(ldcg(in + fr.c0));
+            const Prim<R, DIM> p1 = unpack<R, DIM>(ldcg(in + fr.c1));
+            R flow[NV];
+            if (f < g.nfi) {
+                GradRec<R, DIM> g0, g1;
+                if (REC) {
+                    g0 = ldcg(gr + fr.c0);
+                    g1 = ldcg(gr + fr.c1);
+                }
+                Prim<R, DIM> r[2] = {p0, p1};
+                if (!wf_interior_flux<R, DIM, REC, LIM>(a.flux, r, &g0, &g1, fr, nn, a.gas, flow)) {
+                    flag_error(a.wk.err, a.flux == 2 ? ERR_HLL : ERR_HLLC, f);
 #pragma unroll
-                for (int j = 0; j < NV; ++j) flow[j] = (R)0;
+                    for (int v = 0; v < NV; ++v) flow[v] = (R)0;
+                }
+            } else {
+                boundary_flux<R, DIM>(fr.c0 >= g.nint ? p0 : p1, nn, a.gas, flow);
             }
+            const R S = (R)fr.S;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) o[v] = flow[v] * S;
+            // the time step's terms of this face: products in the reference's
+            // expressions, sums left to the in-order pass below
+            cnj = (sqrt(grm * on.T) + cc) * (R)0.5;
+#pragma unroll
+            for (int k2 = 0; k2 < DIM; ++k2) {
+                const R t = (R)fr2.n[k2];
+                nvj += own.u[k2] * t;
+                pu[k2] = on.u[k2] * t;
+            }
+            sj = (R)fr2.S;
         } else {
-            boundary_flux<R, DIM>(fr.c0 >= g.nint ? p0 : p1, nn, a.gas, flow);
-        }
-        const R S = (R)fr.S;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            const R o = flow[v] * S;  // the face pass's output value
-            if (ent & 1)
-                res[v] += o;
-            else
-                res[v] -= o;
+            for (int v = 0; v < NV; ++v) o[v] = (R)0;
+#pragma unroll
+            for (int k2 = 0; k2 < DIM; ++k2) pu[k2] = (R)0;
+        }
+        // in-order pass over faces r0 .. r0+3 (every lane of the quad)
+        for (int jj = 0; jj < kWfLanes && r0 + jj < K; ++jj) {
+            const int sl = qbase + jj;
+            const int32_t e = __shfl_sync(qmask, ent, sl);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R ov = __shfl_sync(qmask, o[v], sl);
+                if (e & 1)
+                    res[v] += ov;
+                else
+                    res[v] -= ov;
+            }
+#pragma unroll
+            for (int k2 = 0; k2 < DIM; ++k2) nnb += __shfl_sync(qmask, pu[k2], sl);
+            const R nvs = __shfl_sync(qmask, nvj, sl);
+            nnb = (nnb + nvs) * (R)0.5;
+            den += (fabs(nnb) + __shfl_sync(qmask, cnj, sl)) * __shfl_sync(qmask, sj, sl);
         }
     }
-    const Prim<R, DIM> own = unpack<R, DIM>(ldcg(in + c));
-    const double dt = local_time<R, DIM, 1, true, true>(g, in, out, a.gas, a.cfl, 0.0, c, own);
+    if (q != 0) return;
+    const RkIn<NV> rin = rk_load_cg<R, NV>(g, a.wk, first, c);
+    const double dt = (double)((R)a.cfl * (R)g.V[c] / den);
     const CellRec<R> nrec =
         rk_update<R, DIM>(g, a.wk, a.gas, rin, dt, a.alpha[stage], first, stage == a.nst - 1, c, res, sq, mx);
     st16(out + c, nrec);
@@ -229,7 +291,8 @@ __device__ __forceinline__ void wf_item_partials(double sq[NV], double mx[NV], d
     __syncthreads();  // red is reused by the CTA's next item
 }
 
-// Item i at step T (whole CTA; thread t takes the item's t-th cell).
+// Item i at step T (whole CTA; the quad of lanes 4t..4t+3 takes the item's
+// t-th cell).
 template <typename R, int DIM, int REC, int LIM>
 __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i) {
     constexpr int NV = DIM + 2;
@@ -239,16 +302,19 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
     const int j = (int)(m % a.nopi), gofs = a.nopi - a.nst;
     const int64_t k = m / a.nopi;
     const int32_t cb = w.item_ptr[i], ce = w.item_ptr[i + 1];
-    const int32_t c = cb + (int32_t)threadIdx.x < ce ? w.cells[cb + threadIdx.x] : -1;
+    const int slot = (int)threadIdx.x / kWfLanes, q = (int)threadIdx.x % kWfLanes;
+    const int32_t c = cb + slot < ce ? w.cells[cb + slot] : -1;  // the same for the quad
     if (j < gofs) {  // the iteration's gradient
-        if (c >= 0) wf_gradient<R, DIM, REC>(a, k, c);
+        if (c >= 0 && q == 0) wf_gradient<R, DIM, REC>(a, k, c);
         return;
     }
     const int stage = j - gofs;
     double sq[NV], mx[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
-    if (c >= 0) wf_stage_cell<R, DIM, REC, LIM>(a, k * a.nst + stage, k, stage, c, sq, mx);
+    if (c >= 0)
+        wf_stage_quad<R, DIM, REC, LIM>(a, k * a.nst + stage, k, stage, c, q, ((int)threadIdx.x & 31) & ~(kWfLanes - 1),
+                                        sq, mx);
     wf_item_partials<NV>(sq, mx, w.ipart + ((size_t)(m & 1) * w.nitems + i) * 2 * NV);
 }
 
@@ -304,7 +370,7 @@ __device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
 }
 
 template <typename R, int DIM, int REC, int LIM>
-__global__ void __launch_bounds__(kWfBlock, 1) k_wavefront(const __grid_constant__ WfArgs<R> a) {
+__global__ void __launch_bounds__(kWfBlock, DIM == 2 ? PSST_WF_MINB_2D : PSST_WF_MINB_3D) k_wavefront(const __grid_constant__ WfArgs<R> a) {
     constexpr int NV = DIM + 2;
     const WfSched &w = a.sc;
     const int64_t P = w.period;
