@@ -112,27 +112,186 @@ __device__ __forceinline__ bool wf_interior_flux(int flux, Prim<R, DIM> r[2], co
     return interior_flux<R, DIM, 3, REC, LIM>(r, g0, g1, fr, nn, gas, flow);
 }
 
-// Gradient operation of iteration k for cell c (psstFiniteVolumeGrid.cpp:307-308).
+// Gradient (and cell limiter) of cell c by the four lanes of a quad: lane q
+// forms the contributions of the faces q, q+4, .. -- Green-Gauss in the
+// face-loop order (psstGradCalculation.cpp:80-177), least squares in the
+// cell's own order (:268-368; 3D as the corrected restatement of
+// gradient_cell) -- as the products gradient_cell forms, and the quad adds
+// them face by face in that order through shuffles, so the sums are
+// gradient_cell's bit for bit. The neighbour min/max and the Barth-Jespersen
+// / Venkatakrishnan limiter are minima and maxima (order-free). Lane 0 stores
+// the record.
+template <typename R, int DIM, int GRAD, int CELLLIM>
+__device__ __forceinline__ void wf_gradient_quad(const DevGrid &g, const CellRec<R> *rec, GradRec<R, DIM> *gout,
+                                                 int32_t c, int q, int qbase) {
+    constexpr int NVAR = DIM + 2;
+    const unsigned qmask = 0xFu << qbase;
+    const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
+    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    const uint64_t perm = g.wperm[c];
+    const Prim<R, DIM> own = unpack<R, DIM>(ldcg(rec + c));
+    R gr[NVAR][DIM], mx[NVAR], mn[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) {
+        mx[i] = mn[i] = pvar<R, DIM>(own, i);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) gr[i][k] = (R)0;
+    }
+    const double V = g.V[c];
+    constexpr int NR = DIM == 2 ? 3 : 7;
+    R lr[NR], xo[DIM];
+    if (GRAD == 2) {
+#pragma unroll
+        for (int t = 0; t < NR; ++t) lr[t] = (R)g.lsq_r[(int64_t)t * g.nint + c];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) xo[k] = (R)g.xc[(int64_t)k * g.nall + c];
+    }
+    for (int r0 = 0; r0 < K; r0 += kWfLanes) {
+        const int j = r0 + q;
+        R term[NVAR][DIM];
+#pragma unroll
+        for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) term[i][k] = (R)0;
+        if (j < K) {
+            Prim<R, DIM> oth;
+            if (GRAD == 1) {  // face-loop order
+                const int32_t ent = g.csr_ent[b + j];
+                const FaceRec<R, DIM> fr = ldg(frec + (ent >> 1));
+                oth = unpack<R, DIM>(ldcg(rec + g.csr_nb[b + j]));
+                const R beta = (R)g.beta[ent >> 1];
+                const int side = ent & 1;
+                const R rbeta = (R)1 - beta;
+                const R gp = (R)(fr.S / V);
+                const R sgn = side ? (R)1 : (R)-1;
+#pragma unroll
+                for (int i = 0; i < NVAR; ++i) {
+                    const R av = pvar<R, DIM>(own, i), ov = pvar<R, DIM>(oth, i);
+                    const R phi0 = side ? ov : av, phi1 = side ? av : ov;
+                    const R tv = beta * phi0 + rbeta * phi1;
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) term[i][k] = sgn * tv * gp * (R)fr.n[k];
+                }
+            } else {  // the cell's own order
+                const int32_t slot = b + (int32_t)((perm >> (4 * j)) & 15);
+                const int32_t nb = g.csr_nb[slot];
+                oth = unpack<R, DIM>(ldcg(rec + nb));
+                R diff[DIM];
+                R w = (R)0;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    diff[k] = (R)g.xc[(int64_t)k * g.nall + nb] - xo[k];
+                    w += diff[k] * diff[k];
+                }
+                const R ws = (R)1 / w;
+                const R al0 = diff[0] / (lr[0] * lr[0]);
+                const R al1 = (diff[1] - lr[1] / lr[0] * diff[0]) / (lr[2] * lr[2]);
+                R th[DIM];
+                th[0] = al0 - lr[1] / lr[0] * al1;
+                th[1] = al1;
+                if constexpr (DIM == 3) {
+                    const R al2 = (diff[2] - lr[4] / lr[2] * diff[1] + lr[6] * diff[0]) / (lr[5] * lr[5]);
+                    th[0] += al2 * lr[6];
+                    th[1] -= lr[4] / lr[2] * al2;
+                    th[2] = al2;
+                }
+#pragma unroll
+                for (int i = 0; i < NVAR; ++i) {
+                    const R phi = (pvar<R, DIM>(oth, i) - pvar<R, DIM>(own, i));
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) term[i][k] = ws * th[k] * phi;
+                }
+            }
+            if (CELLLIM)
+#pragma unroll
+                for (int i = 0; i < NVAR; ++i) {
+                    const R v = pvar<R, DIM>(oth, i);
+                    if (v > mx[i]) mx[i] = v;
+                    if (v < mn[i]) mn[i] = v;
+                }
+        }
+        for (int jj = 0; jj < kWfLanes && r0 + jj < K; ++jj)
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) gr[i][k] += __shfl_sync(qmask, term[i][k], qbase + jj);
+    }
+    R lim[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) lim[i] = (R)1;
+    if (CELLLIM) {
+#pragma unroll
+        for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+            for (int o = 1; o < kWfLanes; o <<= 1) {
+                const R a = __shfl_xor_sync(qmask, mx[i], o), d = __shfl_xor_sync(qmask, mn[i], o);
+                if (a > mx[i]) mx[i] = a;
+                if (d < mn[i]) mn[i] = d;
+            }
+        const R eps2 = CELLLIM == 5 ? (R)g.vk_eps2[c] : (R)0;
+        for (int j = q; j < K; j += kWfLanes) {
+            const int32_t ent = g.csr_ent[b + j];
+            R off[DIM];
+            face_offsets<R, DIM>(frec + (ent >> 1), ent & 1, off);
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i) {
+                const R phic = pvar<R, DIM>(own, i);
+                R dm = (R)0;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) dm += gr[i][k] * off[k];
+                R pf = (R)1;
+                if (dm != (R)0) {
+                    const R dp = dm > (R)0 ? mx[i] - phic : mn[i] - phic;
+                    if (CELLLIM == 4) {
+                        const R y = dp / dm;
+                        pf = y < (R)1 ? y : (R)1;
+                    } else {
+                        const R num = (dp * dp + eps2) + (R)2 * dm * dp;
+                        const R den = dp * dp + (R)2 * dm * dm + dm * dp + eps2;
+                        pf = num / den;
+                    }
+                }
+                if (pf < lim[i]) lim[i] = pf;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+            for (int o = 1; o < kWfLanes; o <<= 1) {
+                const R a = __shfl_xor_sync(qmask, lim[i], o);
+                if (a < lim[i]) lim[i] = a;
+            }
+    }
+    if (q != 0) return;
+    GradRec<R, DIM> outr;
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) outr.g[i * DIM + k] = CELLLIM ? gr[i][k] * lim[i] : gr[i][k];
+    st16(gout + c, outr);
+}
+
+// Gradient operation of iteration k for cell c (psstFiniteVolumeGrid.cpp:307-308), by a quad.
 template <typename R, int DIM, int REC>
-__device__ __forceinline__ void wf_gradient(const WfArgs<R> &a, int64_t k, int32_t c) {
+__device__ __forceinline__ void wf_gradient(const WfArgs<R> &a, int64_t k, int32_t c, int q, int qbase) {
     const CellRec<R> *in = a.buf[(a.in_buf + k * a.nst) & 1];
     GradRec<R, DIM> *out = reinterpret_cast<GradRec<R, DIM> *>(a.gbuf[(a.n_iter - 1 - k) & 1]);
     if constexpr (REC == 1) {
         if (a.grad == 1)
-            gradient_cell<R, DIM, 1, 0, true>(a.g, in, out, c);
+            wf_gradient_quad<R, DIM, 1, 0>(a.g, in, out, c, q, qbase);
         else
-            gradient_cell<R, DIM, 2, 0, true>(a.g, in, out, c);
+            wf_gradient_quad<R, DIM, 2, 0>(a.g, in, out, c, q, qbase);
     } else if constexpr (REC == 2) {
         if (a.grad == 1) {
             if (a.celllim == 4)
-                gradient_cell<R, DIM, 1, 4, true>(a.g, in, out, c);
+                wf_gradient_quad<R, DIM, 1, 4>(a.g, in, out, c, q, qbase);
             else
-                gradient_cell<R, DIM, 1, 5, true>(a.g, in, out, c);
+                wf_gradient_quad<R, DIM, 1, 5>(a.g, in, out, c, q, qbase);
         } else {
             if (a.celllim == 4)
-                gradient_cell<R, DIM, 2, 4, true>(a.g, in, out, c);
+                wf_gradient_quad<R, DIM, 2, 4>(a.g, in, out, c, q, qbase);
             else
-                gradient_cell<R, DIM, 2, 5, true>(a.g, in, out, c);
+                wf_gradient_quad<R, DIM, 2, 5>(a.g, in, out, c, q, qbase);
         }
     }
 }
@@ -304,8 +463,9 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
     const int32_t cb = w.item_ptr[i], ce = w.item_ptr[i + 1];
     const int slot = (int)threadIdx.x / kWfLanes, q = (int)threadIdx.x % kWfLanes;
     const int32_t c = cb + slot < ce ? w.cells[cb + slot] : -1;  // the same for the quad
+    const int qbase = ((int)threadIdx.x & 31) & ~(kWfLanes - 1);
     if (j < gofs) {  // the iteration's gradient
-        if (c >= 0 && q == 0) wf_gradient<R, DIM, REC>(a, k, c);
+        if (c >= 0) wf_gradient<R, DIM, REC>(a, k, c, q, qbase);
         return;
     }
     const int stage = j - gofs;
@@ -313,8 +473,7 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
     if (c >= 0)
-        wf_stage_quad<R, DIM, REC, LIM>(a, k * a.nst + stage, k, stage, c, q, ((int)threadIdx.x & 31) & ~(kWfLanes - 1),
-                                        sq, mx);
+        wf_stage_quad<R, DIM, REC, LIM>(a, k * a.nst + stage, k, stage, c, q, qbase, sq, mx);
     wf_item_partials<NV>(sq, mx, w.ipart + ((size_t)(m & 1) * w.nitems + i) * 2 * NV);
 }
 
