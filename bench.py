@@ -56,6 +56,11 @@ WORKLOADS = {
     # reference runs the same mesh on one core (it has no Barth-Jespersen: DM/VanLeer there)
     "ramp2d_120x40_fp64": dict(dim=2, mesh=(120, 40), mach=2.5, angle=15.0, precision=64, limiter=4,
                                cpu_mesh=(120, 40), cpu_procs=1),
+    # the 2D case of the configs at its own size in the reference's own evaluation order: 120x40
+    # quads, FP64, MUSCL/Barth-Jespersen, LocalAccTime1 in the reference's in-loop order (one
+    # persistent launch per call); one step = the whole 2000-iteration run
+    "ramp2d_120x40_seq_2000": dict(dim=2, mesh=(120, 40), mach=2.5, angle=15.0, precision=64, limiter=4,
+                                   lc1_mode=0, step_iters=2000, cpu_mesh=(120, 40), cpu_procs=1, cpu_iters=100),
     # the reference's own published case, from its shipped files (tests/golden/shipped_wedge):
     # wedge80_240.msh (19,200 quads), HLL, first order, LocalAccTime1 in the reference's in-loop
     # order, RK1, CFL 2.08; one step = the whole 3000-iteration solve; FP64 (bit-exact with the
@@ -159,7 +164,7 @@ def build_case(workload, directory):
     del mesh
     sc, prim = grid.read_case(directory, "bench")
     sc.precision = w["precision"]
-    sc.lc1_mode = 1
+    sc.lc1_mode = w.get("lc1_mode", 1)
     sc.renumber = 1
     return grid, sc, prim
 
@@ -332,7 +337,9 @@ def scheme_text(workload, cpu=False):
     if w.get("shipped"):
         return "HLL, first order, LocalAccTime1 in the reference's in-loop order, RK1, CFL 2.08 (wedge.inp)"
     lim = "DM/VanLeer" if cpu else ("MUSCL/Venkatakrishnan(K=5)" if w["limiter"] == 5 else "MUSCL/Barth-Jespersen")
-    lc = "LocalAccTime1" if cpu else "LocalAccTime1 (stage-start values)"
+    lc = "LocalAccTime1" if cpu or w.get("lc1_mode") == 0 else "LocalAccTime1 (stage-start values)"
+    if not cpu and w.get("lc1_mode") == 0:
+        lc += " in the reference's in-loop order"
     return "HLLC + %s, Green-Gauss, RK4 std, %s, CFL 0.5, Mach %g, %g deg ramp" % (lim, lc, w["mach"], w["angle"])
 
 
@@ -471,9 +478,10 @@ def run_gpu(args):
     nint = grid.ninterior
     wl = WORKLOADS[args.workload]
     shipped = bool(wl.get("shipped"))
-    # one step: one iteration, or for the published case the whole published solve
-    per_step = int(sc.max_iter) if shipped else 1
-    shapes = solver.autotune(3) if not (args.no_autotune or shipped) else solver.launch_shape()
+    # one step: one iteration, or a whole run (the published solve; the 2000-iteration case)
+    per_step = int(sc.max_iter) if shipped else int(wl.get("step_iters", 1))
+    whole = per_step > 1  # sequential LocalAccTime1: one persistent launch per call
+    shapes = solver.autotune(3) if not (args.no_autotune or whole) else solver.launch_shape()
     # replay whole explicit_solve calls as CUDA graphs (no launch gaps between
     # the passes; on small meshes launch latency dominates); the published case
     # runs as one persistent launch per call (sequential LocalAccTime1)
@@ -489,7 +497,7 @@ def run_gpu(args):
 
     # warm-up
     solver.explicit_solve(args.warmup * per_step)
-    if solver.graphs_on and not shipped:  # capture the timed call's graphs (one per buffer parity) outside the timed region
+    if solver.graphs_on and not whole:  # capture the timed call's graphs (one per buffer parity) outside the timed region
         solver.explicit_solve(args.steps * per_step)
         solver.explicit_solve(args.steps * per_step)
         solver.explicit_solve(per_step)
@@ -511,7 +519,7 @@ def run_gpu(args):
         host_out = torch.empty_like(host_prim).pin_memory()
         barrier()
         t0 = time.perf_counter()
-        if shipped:  # each step: the published solve from its initial state, host to host
+        if whole:  # each step: the whole run from its initial state, host to host
             for _ in range(args.steps):
                 solver.set_state(host_prim.numpy())
                 solver.explicit_solve(per_step)
@@ -527,12 +535,12 @@ def run_gpu(args):
     ms_max, e2e_max = max_over_ranks([ms, e2e_s], ws, "cuda")
     value, e2e_value = replica_throughput(ws, nint * per_step, args.steps, ms_max, e2e_max)
     # per-kernel timing for the roofline (CUDA events around each launch)
-    prof = solver.profile(2 * per_step if shipped else 2)
+    prof = solver.profile(2 * per_step if whole else 2)
     nnz = 2 * grid.nface - grid.nghost  # CSR entries: interior faces twice, boundary faces once
     kernel, (kms, kcnt) = max(prof.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = peaks()
     finite = bool(np.all(np.isfinite(linf))) and bool(np.all(np.isfinite(out)))
-    if shipped:
+    if whole:
         info = solver.schedule_info()
         nopi = sc.rk_level + (1 if sc.order == 2 else 0)
         nsteps = info["period"] * (2 * per_step * nopi - 1) + info["levels"] + 1  # of the profiled call
@@ -570,27 +578,28 @@ def run_gpu(args):
                                      if wl["precision"] == 32 else "FP64 throughout (the parity path)"),
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "threads_per_block": shapes,
-                       "cuda_graphs": args.graphs == "on" and not shipped,
+                       "cuda_graphs": args.graphs == "on" and not whole,
                        "l2_flush": ("not needed: >2.5 GB of mesh + state per step, L2 is 126 MB" if wl["dim"] == 3
                                     else "none: this small case stays in L2 (not the bandwidth benchmark)")},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": state_bytes if shipped else state_bytes / args.steps,
-                    "d2h_bytes_per_step": (state_bytes + per_step * 2 * nv * 8 + 16) if shipped else
+                    "h2d_bytes_per_step": state_bytes if whole else state_bytes / args.steps,
+                    "d2h_bytes_per_step": (state_bytes + per_step * 2 * nv * 8 + 16) if whole else
                                           (state_bytes / args.steps) + 2 * nv * 8 + 16,
                     "note": ("per step: set_state from pinned host memory, one psst_explicit_solve of the %d "
                              "iterations returning every residual column, get_state into pinned host memory; "
-                             "all timed" % per_step) if shipped else
+                             "all timed" % per_step) if whole else
                             "set_state from pinned host memory + K psst_explicit_solve(1) calls each returning "
                             "residual columns + get_state into pinned host memory, all timed"},
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": roof,
-            "kernel_ms_per_iteration": {k: v[0] / (2 * per_step if shipped else 2) for k, v in prof.items()},
+            "kernel_ms_per_iteration": {k: v[0] / (2 * per_step if whole else 2) for k, v in prof.items()},
             "library_device_ms": lib_ms,
             "finite": finite,
         }
+        if whole:
+            line["config"]["step"] = "the whole run: %d iterations of %d cells" % (per_step, nint)
         if shipped:
-            line["config"]["step"] = "the published solve: %d iterations of %d cells" % (per_step, nint)
             line["config"]["published"] = {"wall_s": 152.856, "cell_updates_per_s": PUBLISHED_SHIPPED,
                                            "hardware": "authors' PC, one thread (README)"}
         line.update(extra)
