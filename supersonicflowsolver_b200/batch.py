@@ -125,6 +125,30 @@ def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chu
             "cell_iterations": a["cell_iterations"] + b["cell_iterations"], "threads_per_block": shapes}
 
 
+def unconverged_summary(cases, iterations):
+    """Where the cases that never reach the drop sit: counts (converged / all)
+    per Mach and ramp-angle bin and per mesh size, and the list of the
+    unconverged cases."""
+    mach_edges, angle_edges = [1.8, 2.35, 2.9, 3.45, 4.0], [5.0, 10.0, 15.0, 20.0]
+    grid = {}
+    for c, it in zip(cases, iterations):
+        mb = min(int(np.searchsorted(mach_edges, c["mach"], side="right")) - 1, len(mach_edges) - 2)
+        ab = min(int(np.searchsorted(angle_edges, c["angle"], side="right")) - 1, len(angle_edges) - 2)
+        key = "M %.2f-%.2f, %g-%g deg" % (mach_edges[mb], mach_edges[mb + 1], angle_edges[ab], angle_edges[ab + 1])
+        g = grid.setdefault(key, [0, 0])
+        g[1] += 1
+        g[0] += it is not None
+    sizes = {}
+    for c, it in zip(cases, iterations):
+        k = "%dx%d" % (c["nx"], c["ny"])
+        g = sizes.setdefault(k, [0, 0])
+        g[1] += 1
+        g[0] += it is not None
+    bad = [dict(c, index=i) for i, (c, it) in enumerate(zip(cases, iterations)) if it is None]
+    return {"by_mach_angle": {k: "%d/%d" % tuple(v) for k, v in sorted(grid.items())},
+            "by_mesh": {k: "%d/%d" % tuple(v) for k, v in sorted(sizes.items())}, "unconverged": bad}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--cases", type=int, default=256)
@@ -159,7 +183,8 @@ def main():
                           "iterations_median": float(np.median(its)) if its else None,
                           "iterations_max": max(its) if its else None,
                           "fp32_iterations_median": float(np.median(f32)) if f32 else None,
-                          "fp64_iterations_median": float(np.median(f64)) if f64 else None}))
+                          "fp64_iterations_median": float(np.median(f64)) if f64 else None,
+                          "where": unconverged_summary(cases, r["iterations"])}))
         return
     with tempfile.TemporaryDirectory() as d:
         t0 = time.perf_counter()
@@ -178,7 +203,8 @@ def main():
            "wall_s": r["wall_s"], "device_s": r["device_s"],
            "cell_updates_per_s": r["cell_iterations"] / r["wall_s"],
            "iterations_median": float(np.median(its)) if its else None,
-           "iterations_max": max(its) if its else None}
+           "iterations_max": max(its) if its else None,
+           "where": unconverged_summary(cases, r["iterations"])}
     print(json.dumps(out))
 
 
