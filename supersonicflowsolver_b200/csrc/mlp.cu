@@ -153,7 +153,7 @@ __device__ __forceinline__ void stage(bf16 *s, const bf16 *g, int64_t sr, int64_
                                       int kend) {
     if (sk == 1 && (sr % 8) == 0 && ((uintptr_t)g & 15) == 0) {
         for (int i = threadIdx.x; i < ROWS * 8; i += kThreads) {
-            const int r = i % ROWS, kc = i / ROWS;
+            const int r = i / 8, kc = i % 8;  // eight lanes read one row's 128 bytes
             const int k = k0 + kc * 8;
             int4 v = make_int4(0, 0, 0, 0);
             if (r0 + r < nrows && k < kend) {
