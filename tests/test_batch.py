@@ -206,3 +206,16 @@ def test_device_stop_rule_stops_each_case_at_its_own_iteration(tmp_path):
     state = b.get_state()
     for i in range(3):
         assert np.array_equal(case_part(state, m, i, 4), solo_state[i]), "case %d" % i
+
+
+def test_unconverged_summary_bins_every_case():
+    from supersonicflowsolver_b200 import batch as bt
+
+    cases = bt.sample_cases(64, seed=3)
+    its = [None if c["angle"] > 15.0 else 100 for c in cases]
+    w = bt.unconverged_summary(cases, its)
+    tot = sum(int(v.split("/")[1]) for v in w["by_mach_angle"].values())
+    ok = sum(int(v.split("/")[0]) for v in w["by_mach_angle"].values())
+    assert tot == 64 and ok == sum(i is not None for i in its)
+    assert sum(int(v.split("/")[1]) for v in w["by_mesh"].values()) == 64
+    assert {c["index"] for c in w["unconverged"]} == {i for i, x in enumerate(its) if x is None}
