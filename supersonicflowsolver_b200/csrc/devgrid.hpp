@@ -161,7 +161,7 @@ struct WfSched {
     double *acc;                // [nacc][2 NV] per RK stage: the same over the levels folded so far
     int32_t nacc;
     void *grec2;                // second gradient buffer (gradients by iteration parity)
-    unsigned *sync;             // [4] grid barrier: arrivals, generation, abort flag
+    unsigned *sync;             // grid barrier: arrivals, generation, abort flag (one 128-byte line each)
 };
 
 template <typename R>

@@ -672,7 +672,7 @@ template <typename R>
 void wavefront_run(psst_solver *s, int n_iter) {
     DevState<R> *st = states<R>(s);
     DevWork<R> &w = work<R>(s);
-    ck(cudaMemsetAsync(s->wf.sync, 0, 4 * sizeof(unsigned), s->stream), "memset");
+    ck(cudaMemsetAsync(s->wf.sync, 0, kWfSyncWords * sizeof(unsigned), s->stream), "memset");
     WfArgs<R> a{};
     a.g = s->g;
     a.buf[0] = st[0].rec;
@@ -1214,7 +1214,7 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
             w.acc = s->dalloc<double>((size_t)w.nacc * 2 * s->nv);
             w.grec2 = s->dalloc_bytes(Ops<double>::grad_rec_bytes(s->dim) * std::max(L.nint, 1));
             ck(cudaMemset(w.grec2, 0, Ops<double>::grad_rec_bytes(s->dim) * std::max(L.nint, 1)), "memset");
-            w.sync = s->dalloc<unsigned>(4);
+            w.sync = s->dalloc<unsigned>(kWfSyncWords);
             s->wf_ready = true;
         }
     }

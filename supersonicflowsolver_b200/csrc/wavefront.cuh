@@ -53,10 +53,14 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Grid barrier of a cooperative launch (all CTAs co-resident). sync[0]
-// counts arrivals, sync[1] is the generation, sync[2] the abort flag. The
-// last CTA to arrive resets the count and releases the next generation; the
-// others poll it for at most wait_ns (0: not at all). Returns false when the
-// launch is aborted (here or in another CTA).
+// counts arrivals, sync[kSyncGen] is the generation, sync[kSyncAbort] the
+// abort flag, each on its own 128-byte line so that the CTAs polling the
+// generation do not slow the arrivals' atomics. The last CTA to arrive resets
+// the count and releases the next generation; the others poll it for at most
+// wait_ns (0: not at all). Returns false when the launch is aborted (here or
+// in another CTA).
+constexpr int kSyncGen = 32, kSyncAbort = 64;
+static_assert(kSyncAbort < kWfSyncWords, "barrier words");
 __device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned &gen, uint64_t wait_ns, int32_t *err,
                                              int64_t step) {
     __shared__ int s_go;
@@ -67,24 +71,24 @@ __device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned &gen, uint
         __threadfence();  // this CTA's writes (ordered before by the CTA barrier) before its arrival
         if (atomicAdd(&sync[0], 1u) == gridDim.x - 1) {
             sync[0] = 0u;
-            st_release_gpu(&sync[1], g0 + 1u);
+            st_release_gpu(&sync[kSyncGen], g0 + 1u);
         } else {
             const uint64_t t0 = global_ns();
             for (;;) {
-                if (ld_acquire_gpu(&sync[1]) != g0) break;
-                if (ld_acquire_gpu(&sync[2]) != 0u) {
+                if (ld_acquire_gpu(&sync[kSyncGen]) != g0) break;
+                if (ld_acquire_gpu(&sync[kSyncAbort]) != 0u) {
                     go = 0;
                     break;
                 }
                 if (wait_ns == 0 || global_ns() - t0 > wait_ns) {
-                    atomicExch(&sync[2], 1u);
+                    atomicExch(&sync[kSyncAbort], 1u);
                     flag_error(err, ERR_TIMEOUT, (int)step);
                     go = 0;
                     break;
                 }
             }
         }
-        if (go && ld_acquire_gpu(&sync[2]) != 0u) go = 0;
+        if (go && ld_acquire_gpu(&sync[kSyncAbort]) != 0u) go = 0;
         gen = g0 + 1u;
         s_go = go;
     }
