@@ -481,12 +481,11 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
     wf_item_partials<NV>(sq, mx, w.ipart + ((size_t)(m & 1) * w.nitems + i) * 2 * NV);
 }
 
-// After the barrier that ends step T: folds the item partials of the levels
-// completed at step T into their stage's running norms, in level order; the
-// last level finishes the stage: RMS and max folded into the iteration's
-// columns as max over stages (the columns of k_norm_finish). The completed
-// levels (each of another stage) are spread over all CTAs; a stage's running
-// sums pass from CTA to CTA across steps, so they are read through L2.
+// Block 0, after the barrier that ends step T: folds the item partials of the
+// levels completed at step T into their stage's running norms, in level order;
+// the last level finishes the stage: RMS and max folded into the iteration's
+// columns as max over stages (the columns of k_norm_finish). (Spreading the
+// levels over all CTAs, a thread each, measured three times slower per step.)
 template <typename R, int NV>
 __device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
     const WfSched &w = a.sc;
@@ -496,9 +495,7 @@ __device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
     const int64_t lhi = r + (lmax - r) / P * P;
     const int64_t t0 = T - P * (a.nops - 1);
     const int64_t llo = t0 > r ? t0 : r;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t n = blockIdx.x + (int64_t)gridDim.x * threadIdx.x; llo + P * n <= lhi; n += stride) {
-        const int64_t l = llo + P * n;
+    for (int64_t l = llo + P * (int64_t)threadIdx.x; l <= lhi; l += P * (int64_t)blockDim.x) {
         const int64_t m = (T - l) / P;
         const int j = (int)(m % a.nopi), gofs = a.nopi - a.nst;
         if (j < gofs) continue;  // gradient operation: no residual
@@ -520,8 +517,8 @@ __device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
                 acc[v] = sum[v];
                 acc[NV + v] = mx[v];
             } else {
-                acc[v] = ldcg(acc + v) + sum[v];
-                acc[NV + v] = fmax(ldcg(acc + NV + v), mx[v]);
+                acc[v] += sum[v];
+                acc[NV + v] = fmax(acc[NV + v], mx[v]);
             }
         }
         if (l == w.nlevels - 1) {
@@ -529,9 +526,8 @@ __device__ __forceinline__ void wf_fold(const WfArgs<R> &a, int64_t T) {
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const double rms = sqrt(acc[v] / (double)(a.g.nint > 0 ? a.g.nint : 1));
-                const double l2o = ldcg(a.wk.l2 + it * NV + v), lio = ldcg(a.wk.linf + it * NV + v);
-                if (rms > l2o) a.wk.l2[it * NV + v] = rms;
-                if (lio < acc[NV + v]) a.wk.linf[it * NV + v] = acc[NV + v];
+                if (rms > a.wk.l2[it * NV + v]) a.wk.l2[it * NV + v] = rms;
+                if (a.wk.linf[it * NV + v] < acc[NV + v]) a.wk.linf[it * NV + v] = acc[NV + v];
             }
         }
     }
@@ -545,7 +541,7 @@ __global__ void __launch_bounds__(kWfBlock, DIM == 2 ? PSST_WF_MINB_2D : PSST_WF
     const int64_t tend = P * (a.nops - 1) + w.nlevels + 1;
     unsigned gen = 0;
     for (int64_t T = 0; T < tend; ++T) {
-        if (T > 0) wf_fold<R, NV>(a, T - 1);
+        if (blockIdx.x == 0 && T > 0) wf_fold<R, NV>(a, T - 1);
         // items of step T: levels l = T (mod P) whose operation (T - l) / P is in [0, nops)
         const int64_t r = T % P;
         const int64_t lmax = T < w.nlevels - 1 ? T : (int64_t)w.nlevels - 1;
