@@ -1199,8 +1199,9 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
         alloc_state<double>(s.get(), *G);
     if (s->seq && sc->precision == 64 && L.cell_case.empty() && !L.wf_item_level.empty()) {
         const int maxb = Ops<double>::wavefront_max_blocks(s->dim, s->rec, sc->limiter);
-        s->wf_blocks = std::min(std::max(L.wf_max_class_items, 2), maxb);
-        if (s->wf_blocks >= 2) {  // one CTA would never wait: the barrier needs two
+        // CTA 0 folds the norms; the others take the work items of a step
+        s->wf_blocks = std::min(L.wf_max_class_items + 1, maxb);
+        if (s->wf_blocks >= 2) {  // the items need a CTA besides CTA 0
             WfSched &w = s->wf;
             w.period = L.wf_period;
             w.nlevels = L.nlevels;

@@ -481,8 +481,9 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
     wf_item_partials<NV>(sq, mx, w.ipart + ((size_t)(m & 1) * w.nitems + i) * 2 * NV);
 }
 
-// Block 0, after the barrier that ends step T: folds the item partials of the
-// levels completed at step T into their stage's running norms, in level order;
+// Block 0 (which takes no work items), after the barrier that ends step T:
+// folds the item partials of the levels completed at step T into their
+// stage's running norms, in level order;
 // the last level finishes the stage: RMS and max folded into the iteration's
 // columns as max over stages (the columns of k_norm_finish). (Spreading the
 // levels over all CTAs, a thread each, measured three times slower per step.)
@@ -549,9 +550,9 @@ __global__ void __launch_bounds__(kWfBlock, DIM == 2 ? PSST_WF_MINB_2D : PSST_WF
             const int64_t lhi = r + (lmax - r) / P * P;
             const int64_t t0 = T - P * (a.nops - 1);
             const int64_t llo = t0 > r ? t0 : r;
-            if (llo <= lhi) {
+            if (llo <= lhi && blockIdx.x > 0) {  // CTA 0 folds the norms instead
                 const int32_t i0 = w.lvl_items[2 * llo], i1 = w.lvl_items[2 * lhi + 1];
-                for (int32_t i = i0 + (int32_t)blockIdx.x; i < i1; i += (int32_t)gridDim.x)
+                for (int32_t i = i0 + (int32_t)blockIdx.x - 1; i < i1; i += (int32_t)gridDim.x - 1)
                     wf_item<R, DIM, REC, LIM>(a, T, i);
             }
         }
