@@ -153,8 +153,9 @@ struct CaseStop {
 struct WfSched {
     int32_t period;          // P
     int32_t nlevels, nitems;
-    const int32_t *cells;       // [nint] interior cells in item order
-    const int32_t *item_ptr;    // [nitems+1] cell range of each item in `cells`
+    const int32_t *cells32;     // [nitems][32] the cells of each item (-1: empty slot)
+    const uint32_t *lowmask;    // [nint] bit q: the cell across CSR entry q was updated
+                                // before this cell in the reference's order
     const int32_t *item_level;  // [nitems]
     const int32_t *lvl_items;   // [2 nlevels] item range [first, end) of each level
     double *ipart;              // [2][nitems][2 NV] per item: sum res^2, max |res| (by operation parity)

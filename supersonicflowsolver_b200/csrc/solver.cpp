@@ -78,7 +78,8 @@ struct Layout {
     std::vector<int32_t> c0, c1, csr_ptr, csr_ent, csr_nb, rank, gptr, g_nb, g_face, g_zone, z_dyn, z_therm, lvl_cells, lvl_ptr;
     // wavefront schedule of the sequential LocalAccTime1 (WfSched)
     int32_t wf_period = 1, wf_max_class_items = 0;
-    std::vector<int32_t> wf_cells, wf_item_ptr, wf_item_level, wf_lvl_items;
+    std::vector<int32_t> wf_cells32, wf_item_level, wf_lvl_items;
+    std::vector<uint32_t> wf_lowmask;
     std::vector<uint64_t> wperm;
     std::vector<double> S, n, xf, beta, V, xc, lsq_r, vk_eps2, z_u, z_p, z_T;
 };
@@ -356,25 +357,29 @@ void build_layout(const psst_grid &G, const psst_scheme &sc, Layout &L) {
         std::vector<int32_t> by_level(L.nint), fill(L.lvl_ptr.begin(), L.lvl_ptr.end() - 1);
         for (int32_t d = 0; d < L.nint; ++d) by_level[fill[level[d]]++] = d;
         L.wf_lvl_items.assign((size_t)2 * L.nlevels, 0);
-        L.wf_cells.clear();
-        L.wf_item_ptr.clear();
+        L.wf_cells32.clear();
         L.wf_item_level.clear();
+        const int32_t per_item = kWfBlock / kWfLanes;
         for (int32_t r = 0; r < L.wf_period; ++r) {
             const int32_t first = (int32_t)L.wf_item_level.size();
             for (int32_t l = r; l < L.nlevels; l += L.wf_period) {
                 L.wf_lvl_items[2 * (size_t)l] = (int32_t)L.wf_item_level.size();
-                const int32_t per_item = kWfBlock / kWfLanes;
                 for (int32_t b = L.lvl_ptr[l]; b < L.lvl_ptr[l + 1]; b += per_item) {
-                    L.wf_item_ptr.push_back((int32_t)L.wf_cells.size());
                     L.wf_item_level.push_back(l);
-                    for (int32_t i = b; i < std::min(b + per_item, L.lvl_ptr[l + 1]); ++i)
-                        L.wf_cells.push_back(by_level[i]);
+                    for (int32_t i = b; i < b + per_item; ++i)
+                        L.wf_cells32.push_back(i < L.lvl_ptr[l + 1] ? by_level[i] : -1);
                 }
                 L.wf_lvl_items[2 * (size_t)l + 1] = (int32_t)L.wf_item_level.size();
             }
             L.wf_max_class_items = std::max(L.wf_max_class_items, (int32_t)L.wf_item_level.size() - first);
         }
-        L.wf_item_ptr.push_back((int32_t)L.wf_cells.size());
+        // neighbours updated before each cell in the reference's order, per CSR entry
+        L.wf_lowmask.assign(L.nint, 0u);
+        for (int32_t d = 0; d < L.nint; ++d)
+            for (int32_t q = L.csr_ptr[d]; q < L.csr_ptr[d + 1]; ++q) {
+                const int32_t nb = L.csr_nb[q];
+                if (nb < L.nint && L.rank[nb] < L.rank[d]) L.wf_lowmask[d] |= 1u << (q - L.csr_ptr[d]);
+            }
     }
 }
 
@@ -1206,8 +1211,8 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
             w.period = L.wf_period;
             w.nlevels = L.nlevels;
             w.nitems = (int32_t)L.wf_item_level.size();
-            w.cells = s->upload(L.wf_cells);
-            w.item_ptr = s->upload(L.wf_item_ptr);
+            w.cells32 = s->upload(L.wf_cells32);
+            w.lowmask = s->upload(L.wf_lowmask);
             w.item_level = s->upload(L.wf_item_level);
             w.lvl_items = s->upload(L.wf_lvl_items);
             w.ipart = s->dalloc<double>((size_t)2 * w.nitems * 2 * s->nv);

@@ -131,7 +131,7 @@ __device__ __forceinline__ void wf_gradient_quad(const DevGrid &g, const CellRec
     constexpr int NVAR = DIM + 2;
     const unsigned qmask = 0xFu << qbase;
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
-    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    const int32_t b = g.kuni ? c * g.kuni : g.csr_ptr[c], K = g.kuni ? g.kuni : g.csr_ptr[c + 1] - b;
     const uint64_t perm = g.wperm[c];
     const Prim<R, DIM> own = unpack<R, DIM>(ldcg(rec + c));
     R gr[NVAR][DIM], mx[NVAR], mn[NVAR];
@@ -322,9 +322,10 @@ __device__ __forceinline__ void wf_stage_quad(const WfArgs<R> &a, int64_t s, int
     const GradRec<R, DIM> *gr = reinterpret_cast<const GradRec<R, DIM> *>(a.gbuf[(a.n_iter - 1 - k) & 1]);
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     const int first = stage == 0;
-    const int32_t b = g.csr_ptr[c], K = g.csr_ptr[c + 1] - b;
+    // uniform meshes (all quads, all tets): the CSR range follows from c
+    const int32_t b = g.kuni ? c * g.kuni : g.csr_ptr[c], K = g.kuni ? g.kuni : g.csr_ptr[c + 1] - b;
     const uint64_t perm = g.wperm[c];
-    const int32_t myrank = g.rank[c];
+    const uint32_t low = a.sc.lowmask[c];
     const Prim<R, DIM> own = unpack<R, DIM>(ldcg(in + c));
     const R grm = (R)a.gas.gamma * (R)a.gas.rm;
     const R cc = sqrt(grm * own.T);
@@ -337,21 +338,25 @@ __device__ __forceinline__ void wf_stage_quad(const WfArgs<R> &a, int64_t s, int
         int32_t ent = 0;
         R o[NV], pu[DIM], nvj = (R)0, cnj = (R)0, sj = (R)0;
         if (j < K) {
-            // flux of the j-th face in face-loop order (the face pass's output value)
+            // flux of the j-th face in face-loop order (the face pass's output value);
+            // the cell across it from the CSR, so the state load does not wait
+            // for the face record
             ent = g.csr_ent[b + j];
             const int32_t f = ent >> 1;
+            const Prim<R, DIM> oth = unpack<R, DIM>(ldcg(in + g.csr_nb[b + j]));
+            // own-order position j: its neighbour for the time step, from this
+            // stage's output if the reference updates it before this cell
+            const int32_t slot2 = (int32_t)((perm >> (4 * j)) & 15);
+            const int32_t ent2 = g.csr_ent[b + slot2];
+            const CellRec<R> *src = ((low >> slot2) & 1u) ? out : in;
+            const Prim<R, DIM> on = unpack<R, DIM>(ldcg(src + g.csr_nb[b + slot2]));
             const FaceRec<R, DIM> fr = ldg(frec + f);
-            // own-order position j: its neighbour for the time step
-            const int32_t ent2 = g.csr_ent[b + (int32_t)((perm >> (4 * j)) & 15)];
             const FaceRec<R, DIM> fr2 = ent2 == ent ? fr : ldg(frec + (ent2 >> 1));
-            const int32_t nb = (ent2 & 1) ? fr2.c0 : fr2.c1;
-            const CellRec<R> *src = (nb < g.nint && g.rank[nb] < myrank) ? out : in;
-            const Prim<R, DIM> on = unpack<R, DIM>(ldcg(src + nb));
             R nn[DIM];
 #pragma unroll
             for (int k2 = 0; k2 < DIM; ++k2) nn[k2] = (R)fr.n[k2];
-            const Prim<R, DIM> p0 = unpack<R, DIM>(ldcg(in + fr.c0));
-            const Prim<R, DIM> p1 = unpack<R, DIM>(ldcg(in + fr.c1));
+            const Prim<R, DIM> p0 = (ent & 1) ? oth : own;  // this cell is neighbour (ent & 1)
+            const Prim<R, DIM> p1 = (ent & 1) ? own : oth;
             R flow[NV];
             if (f < g.nfi) {
                 GradRec<R, DIM> g0, g1;
@@ -366,7 +371,7 @@ __device__ __forceinline__ void wf_stage_quad(const WfArgs<R> &a, int64_t s, int
                     for (int v = 0; v < NV; ++v) flow[v] = (R)0;
                 }
             } else {
-                boundary_flux<R, DIM>(fr.c0 >= g.nint ? p0 : p1, nn, a.gas, flow);
+                boundary_flux<R, DIM>(oth, nn, a.gas, flow);  // the ghost side
             }
             const R S = (R)fr.S;
 #pragma unroll
@@ -464,9 +469,8 @@ __device__ __forceinline__ void wf_item(const WfArgs<R> &a, int64_t T, int32_t i
     const int64_t m = (T - l) / w.period;
     const int j = (int)(m % a.nopi), gofs = a.nopi - a.nst;
     const int64_t k = m / a.nopi;
-    const int32_t cb = w.item_ptr[i], ce = w.item_ptr[i + 1];
     const int slot = (int)threadIdx.x / kWfLanes, q = (int)threadIdx.x % kWfLanes;
-    const int32_t c = cb + slot < ce ? w.cells[cb + slot] : -1;  // the same for the quad
+    const int32_t c = w.cells32[(size_t)i * (kWfBlock / kWfLanes) + slot];  // the same for the quad
     const int qbase = ((int)threadIdx.x & 31) & ~(kWfLanes - 1);
     if (j < gofs) {  // the iteration's gradient
         if (c >= 0) wf_gradient<R, DIM, REC>(a, k, c, q, qbase);
