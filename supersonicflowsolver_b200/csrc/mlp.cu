@@ -151,7 +151,21 @@ struct GemmArgs {
 template <int ROWS>
 __device__ __forceinline__ void stage(bf16 *s, const bf16 *g, int64_t sr, int64_t sk, int r0, int nrows, int k0,
                                       int kend) {
-    if (sk == 1 && (sr % 8) == 0 && ((uintptr_t)g & 15) == 0) {
+    if (sk == 1 && (sr % 8) == 0 && ((uintptr_t)g & 15) == 0 && r0 + ROWS <= nrows && k0 + kChunkK <= kend) {
+        // whole tile in range: every load of the thread issued before any store
+        constexpr int IT = ROWS * 8 / kThreads;
+        int4 v[IT];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int i = threadIdx.x + it * kThreads;
+            v[it] = *reinterpret_cast<const int4 *>(g + (int64_t)(r0 + i / 8) * sr + k0 + (i % 8) * 8);
+        }
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int i = threadIdx.x + it * kThreads;
+            *reinterpret_cast<int4 *>(s + ((size_t)(i % 8) * ROWS + i / 8) * 8) = v[it];
+        }
+    } else if (sk == 1 && (sr % 8) == 0 && ((uintptr_t)g & 15) == 0) {
         for (int i = threadIdx.x; i < ROWS * 8; i += kThreads) {
             const int r = i / 8, kc = i % 8;  // eight lanes read one row's 128 bytes
             const int k = k0 + kc * 8;
