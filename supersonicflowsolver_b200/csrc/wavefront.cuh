@@ -35,6 +35,10 @@
 #ifndef PSST_WF_MINB_3D
 #define PSST_WF_MINB_3D 2
 #endif
+// pause between two polls of the grid barrier's generation (ns)
+#ifndef PSST_WF_POLL_NS
+#define PSST_WF_POLL_NS 32
+#endif
 
 namespace psst {
 
@@ -76,6 +80,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned &gen, uint
             const uint64_t t0 = global_ns();
             for (;;) {
                 if (ld_acquire_gpu(&sync[kSyncGen]) != g0) break;
+                __nanosleep(PSST_WF_POLL_NS);  // fewer polls competing with the arrivals for L2
                 if (ld_acquire_gpu(&sync[kSyncAbort]) != 0u) {
                     go = 0;
                     break;
