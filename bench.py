@@ -481,7 +481,6 @@ def run_gpu(args):
     # one step: one iteration, or a whole run (the published solve; the 2000-iteration case)
     per_step = int(sc.max_iter) if shipped else int(wl.get("step_iters", 1))
     whole = per_step > 1  # sequential LocalAccTime1: one persistent launch per call
-    chunks = solver.set_chunks(args.chunks)
     shapes = solver.autotune(3) if not (args.no_autotune or whole) else solver.launch_shape()
     # replay whole explicit_solve calls as CUDA graphs (no launch gaps between
     # the passes; on small meshes launch latency dominates); the published case
@@ -579,7 +578,6 @@ def run_gpu(args):
                                      if wl["precision"] == 32 else "FP64 throughout (the parity path)"),
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "threads_per_block": shapes,
-                       "face_cell_chunks": chunks,
                        "cuda_graphs": args.graphs == "on" and not whole,
                        "l2_flush": ("not needed: >2.5 GB of mesh + state per step, L2 is 126 MB" if wl["dim"] == 3
                                     else "none: this small case stays in L2 (not the bandwidth benchmark)")},
@@ -630,8 +628,6 @@ def main():
     ap.add_argument("--graphs", choices=["on", "off"], default="on",
                     help="replay each explicit_solve call as a CUDA graph")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
-    ap.add_argument("--chunks", type=int, default=0,
-                    help="face/cell chunk interleave: 0 automatic (the library's default), 1 off, n chunks")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the FP64 line and the FP32-vs-FP64 field error of the 6M-tet workload")
     args = ap.parse_args()

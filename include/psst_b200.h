@@ -286,16 +286,6 @@ psst_status psst_solver_profile(psst_solver *s, int n_iter, double *ms_per_kind,
  * the cell-pass shape). Allocates a state-sized snapshot for the call. */
 psst_status psst_solver_autotune(psst_solver *s, int n_iter, int *blocks);
 
-/* No counterpart in the reference. Face/cell chunk interleave of the parallel
- * modes: each RK stage runs, chunk by chunk, the face pass over the faces whose
- * lower cell is in the chunk and then the cell pass over the chunk's cells,
- * with L2 eviction hints, so the cell pass reads the chunk's face outputs from
- * L2 instead of HBM. chunks: 0 automatic (on when the face outputs do not fit
- * in about half of the L2; the default), 1 off, n > 1 n chunks. Results do not
- * change (the RMS column's block partials keep their blocks). in_use (may be
- * NULL) receives the chunk count now in use (1: no interleave). */
-psst_status psst_solver_set_chunks(psst_solver *s, int chunks, int *in_use);
-
 /* Sets (set != NULL; 0 keeps an entry) and/or reads (get != NULL) the launch
  * shapes {gradient, face, cell}: 64, 128 or 256 threads per block (default
  * 256). */

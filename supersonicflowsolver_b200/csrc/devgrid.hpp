@@ -125,19 +125,6 @@ struct Gas {
     double rm, cp, cv, gamma;
 };
 
-// Faces one face-pass launch covers: interior faces [fi0, fi0 + ni) and
-// boundary faces [fb0, fb0 + nb). interleave: part of a face/cell chunk
-// interleave (L2 eviction hints on the face records and outputs).
-struct FaceRange {
-    int32_t fi0, ni, fb0, nb;
-    int32_t interleave;
-};
-// Cells one cell-pass launch covers, [c0, c1); its block b writes the norm
-// partial of block blk0 + b of the nblk blocks of a whole pass.
-struct CellRange {
-    int32_t c0, c1, blk0, nblk;
-};
-
 // Per-case stop rule of merged grids, evaluated on the device after every
 // iteration: each component of a case's residual column is normalised by its
 // maximum over the case's first scale_iters iterations (or by a given

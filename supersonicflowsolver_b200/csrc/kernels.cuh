@@ -200,62 +200,6 @@ __device__ __forceinline__ void st16(T *p, const T &t) {
     }
 }
 
-// L2 eviction policies (createpolicy) and record loads/stores that carry one:
-// with the face/cell chunk interleave, the face pass streams its face records
-// with evict_first and keeps its outputs with evict_last until the cell pass
-// of the same chunk reads them (and demotes them to evict_normal); otherwise
-// every access carries evict_normal, the default.
-enum L2Pol { L2_NORMAL = 0, L2_FIRST = 1, L2_LAST = 2 };
-__device__ __forceinline__ uint64_t l2_policy(int kind) {
-    uint64_t p;
-    if (kind == L2_LAST)
-        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    else if (kind == L2_FIRST)
-        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    else
-        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-template <typename T>
-__device__ __forceinline__ T ldg_pol(const T *p, uint64_t pol) {
-    static_assert(sizeof(T) % 16 == 0, "record size must be a multiple of 16 bytes");
-    union U {
-        T t;
-        uint32_t w[sizeof(T) / 4];
-        __device__ U() {}
-    } u;
-    const char *q = reinterpret_cast<const char *>(p);
-    constexpr int N32 = (int)(sizeof(T) / 32);
-#pragma unroll
-    for (int i = 0; i < N32; ++i)
-        asm("ld.global.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
-            : "=r"(u.w[8 * i]), "=r"(u.w[8 * i + 1]), "=r"(u.w[8 * i + 2]), "=r"(u.w[8 * i + 3]),
-              "=r"(u.w[8 * i + 4]), "=r"(u.w[8 * i + 5]), "=r"(u.w[8 * i + 6]), "=r"(u.w[8 * i + 7])
-            : "l"(q + 32 * i), "l"(pol));
-    if constexpr (sizeof(T) % 32 != 0)  // a 16-byte tail
-        asm("ld.global.L2::cache_hint.v4.b32 {%0,%1,%2,%3}, [%4], %5;"
-            : "=r"(u.w[8 * N32]), "=r"(u.w[8 * N32 + 1]), "=r"(u.w[8 * N32 + 2]), "=r"(u.w[8 * N32 + 3])
-            : "l"(q + 32 * N32), "l"(pol));
-    return u.t;
-}
-template <typename T>
-__device__ __forceinline__ void st_pol(T *p, const T &t, uint64_t pol) {
-    static_assert(sizeof(T) % 32 == 0, "record size must be a multiple of 32 bytes");
-    union U {
-        T t;
-        uint32_t w[sizeof(T) / 4];
-        __device__ U() {}
-    } u;
-    u.t = t;
-    char *q = reinterpret_cast<char *>(p);
-#pragma unroll
-    for (int i = 0; i < (int)(sizeof(T) / 32); ++i)
-        asm volatile("st.global.L2::cache_hint.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8}, %9;" ::"l"(q + 32 * i),
-                     "r"(u.w[8 * i]), "r"(u.w[8 * i + 1]), "r"(u.w[8 * i + 2]), "r"(u.w[8 * i + 3]),
-                     "r"(u.w[8 * i + 4]), "r"(u.w[8 * i + 5]), "r"(u.w[8 * i + 6]), "r"(u.w[8 * i + 7]), "l"(pol)
-                     : "memory");
-}
-
 // psstScalarLimiters.cpp:17-93
 template <int LIM, typename R>
 __device__ __forceinline__ R limiter_value(R num, R den) {
@@ -535,15 +479,12 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
 //  LocalAccTime2 (:189-193): S |n_k|.
 // Register cap PSST_FACE_MAXNREG on the FP32 path (48: ten 128-thread blocks per SM).
 template <typename R, int DIM, int FLUX, int REC, int LIM, int LC>
-__global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas,
-                                                                          FaceRange rg) {
+__global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGrid g, DevState<R> st, DevWork<R> wk, Gas gas) {
     using FO = FaceOut<R, DIM>;
-    const int32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= rg.ni + rg.nb) return;
-    const int32_t f = idx < rg.ni ? rg.fi0 + idx : rg.fb0 + (idx - rg.ni);
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= g.nface) return;
     if (g.face_case && !g.case_active[g.face_case[f]]) return;  // stopped case (merged grids)
-    const FaceRec<R, DIM> fr = ldg_pol(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f,
-                                       l2_policy(rg.interleave ? L2_FIRST : L2_NORMAL));
+    const FaceRec<R, DIM> fr = ldg(reinterpret_cast<const FaceRec<R, DIM> *>(g.frec) + f);
     R nn[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) nn[k] = (R)fr.n[k];
@@ -595,7 +536,7 @@ __global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGr
 #pragma unroll
         for (int k = 0; k < DIM; ++k) o.v[FO::Q0 + k] = S * fabs(nn[k]);
     }
-    st_pol(reinterpret_cast<FO *>(wk.fout) + f, o, l2_policy(rg.interleave ? L2_LAST : L2_NORMAL));
+    st16(reinterpret_cast<FO *>(wk.fout) + f, o);
 }
 
 // ---------------------------------------------------------------------------
@@ -1253,20 +1194,19 @@ __device__ __forceinline__ R lc1_normal_velocities(const FaceOut<R, DIM> &o, int
 template <typename R, int DIM, int LC, bool BATCH>
 __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell(DevGrid g, DevState<R> cur, DevState<R> nxt, DevWork<R> wk, Gas gas,
                                               double cfl, double dt_uniform, double alpha, int stage,
-                                              int kstage, int it_slot, CellRange rg) {
+                                              int kstage, int it_slot) {
     // stage: bit 0 first stage of the iteration, bit 1 last stage; kstage: its index
     using FO = FaceOut<R, DIM>;
     const int first_stage = stage & 1;
     constexpr int NV = DIM + 2;
-    const int32_t c = rg.c0 + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    const uint64_t fpol = l2_policy(L2_NORMAL);  // face outputs: demoted to normal once read
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     __shared__ unsigned warps_done;  // lastwarp_partials
     if (threadIdx.x == 0) warps_done = 0u;
     __syncthreads();
     double sq[NV], mx[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) sq[v] = mx[v] = 0.0;
-    bool run = c < rg.c1;
+    bool run = c < g.nint;
     if (BATCH && run && !g.case_active[g.cell_case[c]]) {  // stopped case: carry the state over
         run = false;
         st16(nxt.rec + c, ldg(cur.rec + c));
@@ -1319,8 +1259,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
 #pragma unroll
                 for (int q = 0; q < 4; ++q) sa[q] = csr_s[b + q];
             }
-            const FO o0 = ldg_pol(fo + (e4.x >> 1), fpol), o1 = ldg_pol(fo + (e4.y >> 1), fpol),
-                     o2 = ldg_pol(fo + (e4.z >> 1), fpol), o3 = ldg_pol(fo + (e4.w >> 1), fpol);
+            const FO o0 = ldg(fo + (e4.x >> 1)), o1 = ldg(fo + (e4.y >> 1)), o2 = ldg(fo + (e4.z >> 1)),
+                     o3 = ldg(fo + (e4.w >> 1));
             entry(e4.x, o0, sa[0]);
             entry(e4.y, o1, sa[1]);
             entry(e4.z, o2, sa[2]);
@@ -1329,7 +1269,7 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
 #pragma unroll 4
             for (int32_t q = 0; q < K; ++q) {
                 const int32_t ent = g.csr_ent[b + q];
-                entry(ent, ldg_pol(fo + (ent >> 1), fpol), csr_s[b + q]);
+                entry(ent, ldg(fo + (ent >> 1)), csr_s[b + q]);
             }
         }
         double dt = dt_uniform;
@@ -1372,8 +1312,8 @@ __global__ void __launch_bounds__(256, PSST_BUDGET(R, PSST_CELL_MINB, 2)) k_cell
         }
     }
     if (BATCH) case_max<NV>(wk.case_linf + (int64_t)it_slot * g.ncase * NV, run ? g.cell_case[c] : -1, mx);
-    lastwarp_partials<NV, sizeof(R) == 4>(
-        sq, mx, wk.l2part + ((int64_t)kstage * rg.nblk + rg.blk0 + blockIdx.x) * 2 * NV, &warps_done);
+    lastwarp_partials<NV, sizeof(R) == 4>(sq, mx, wk.l2part + ((int64_t)kstage * gridDim.x + blockIdx.x) * 2 * NV,
+                                          &warps_done);
 }
 
 // Thread-per-cell update reading the face outputs (GATHER) or the residual of

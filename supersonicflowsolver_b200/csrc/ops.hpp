@@ -43,16 +43,13 @@ struct Ops {
                          const DevWork<R> &wk, cudaStream_t s);
     // face pass: rec 0 first order, 1 DM with limiter lim (1..3), 2 cell-limited
     // MUSCL; lc selects the time-step terms written with each face's flux
-    // (range: a face chunk of the face/cell interleave; null: every face)
     static void face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st,
-                     const DevWork<R> &wk, const Gas &gas, cudaStream_t s, const FaceRange *range = nullptr);
+                     const DevWork<R> &wk, const Gas &gas, cudaStream_t s);
     // cell pass of the parallel modes (lc 0, 2, 1 from stage-start values):
     // residual, time step, RK update, ghosts, block norm partials of stage kstage
-    // (range: a cell chunk of the interleave, c0 a multiple of 256; null: every cell)
     static void cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                      const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha,
-                     int stage, int kstage, int it_slot, cudaStream_t s,
-                     const CellRange *range = nullptr);  // stage: 1 first, 2 last (bits)
+                     int stage, int kstage, int it_slot, cudaStream_t s);  // stage: 1 first, 2 last (bits)
     // the iteration's residual columns from the cell passes' partials of nstage stages
     static void norm_reduce(int dim, const DevGrid &g, const DevWork<R> &wk, int nstage, int it_slot,
                             cudaStream_t s);

@@ -103,93 +103,83 @@ void Ops<R>::gradient(int dim, int grad, int celllim, const DevGrid &g, const De
 // ---- face pass: DIM x FLUX x (REC, LIM) x LC ----
 template <typename R, int DIM, int FLUX, int REC, int LIM>
 static void face_l(int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk, const Gas &gas,
-                   const FaceRange &rg, cudaStream_t s) {
-    const int bs = g.blk_face, nb = nblocks((int64_t)rg.ni + rg.nb, bs);
-    if (nb == 0) return;
+                   cudaStream_t s) {
+    const int bs = g.blk_face, nb = nblocks(g.nface, bs);
     if (lc == 1)
-        k_face<R, DIM, FLUX, REC, LIM, 1><<<nb, bs, 0, s>>>(g, st, wk, gas, rg);
+        k_face<R, DIM, FLUX, REC, LIM, 1><<<nb, bs, 0, s>>>(g, st, wk, gas);
     else if (lc == 2)
-        k_face<R, DIM, FLUX, REC, LIM, 2><<<nb, bs, 0, s>>>(g, st, wk, gas, rg);
+        k_face<R, DIM, FLUX, REC, LIM, 2><<<nb, bs, 0, s>>>(g, st, wk, gas);
     else
-        k_face<R, DIM, FLUX, REC, LIM, 0><<<nb, bs, 0, s>>>(g, st, wk, gas, rg);
+        k_face<R, DIM, FLUX, REC, LIM, 0><<<nb, bs, 0, s>>>(g, st, wk, gas);
 }
 
 template <typename R, int DIM, int FLUX>
 static void face_r(int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
-                   const Gas &gas, const FaceRange &rg, cudaStream_t s) {
+                   const Gas &gas, cudaStream_t s) {
     if (rec == 0)
-        face_l<R, DIM, FLUX, 0, 1>(lc, g, st, wk, gas, rg, s);
+        face_l<R, DIM, FLUX, 0, 1>(lc, g, st, wk, gas, s);
     else if (rec == 2)
-        face_l<R, DIM, FLUX, 2, 1>(lc, g, st, wk, gas, rg, s);
+        face_l<R, DIM, FLUX, 2, 1>(lc, g, st, wk, gas, s);
     else if (lim == 1)
-        face_l<R, DIM, FLUX, 1, 1>(lc, g, st, wk, gas, rg, s);
+        face_l<R, DIM, FLUX, 1, 1>(lc, g, st, wk, gas, s);
     else if (lim == 2)
-        face_l<R, DIM, FLUX, 1, 2>(lc, g, st, wk, gas, rg, s);
+        face_l<R, DIM, FLUX, 1, 2>(lc, g, st, wk, gas, s);
     else
-        face_l<R, DIM, FLUX, 1, 3>(lc, g, st, wk, gas, rg, s);
+        face_l<R, DIM, FLUX, 1, 3>(lc, g, st, wk, gas, s);
 }
 
 template <typename R, int DIM>
 static void face_f(int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st, const DevWork<R> &wk,
-                   const Gas &gas, const FaceRange &rg, cudaStream_t s) {
+                   const Gas &gas, cudaStream_t s) {
     if (flux == 1)
-        face_r<R, DIM, 1>(rec, lim, lc, g, st, wk, gas, rg, s);
+        face_r<R, DIM, 1>(rec, lim, lc, g, st, wk, gas, s);
     else if (flux == 2)
-        face_r<R, DIM, 2>(rec, lim, lc, g, st, wk, gas, rg, s);
+        face_r<R, DIM, 2>(rec, lim, lc, g, st, wk, gas, s);
     else
-        face_r<R, DIM, 3>(rec, lim, lc, g, st, wk, gas, rg, s);
+        face_r<R, DIM, 3>(rec, lim, lc, g, st, wk, gas, s);
 }
 
 template <typename R>
 void Ops<R>::face(int dim, int flux, int rec, int lim, int lc, const DevGrid &g, const DevState<R> &st,
-                  const DevWork<R> &wk, const Gas &gas, cudaStream_t s, const FaceRange *range) {
+                  const DevWork<R> &wk, const Gas &gas, cudaStream_t s) {
     if (g.nface == 0) return;
-    const FaceRange all{0, g.nfi, g.nfi, g.nface - g.nfi, 0};
-    const FaceRange &rg = range ? *range : all;
     if (dim == 2)
-        face_f<R, 2>(flux, rec, lim, lc, g, st, wk, gas, rg, s);
+        face_f<R, 2>(flux, rec, lim, lc, g, st, wk, gas, s);
     else
-        face_f<R, 3>(flux, rec, lim, lc, g, st, wk, gas, rg, s);
+        face_f<R, 3>(flux, rec, lim, lc, g, st, wk, gas, s);
 }
 
 // ---- cell pass (parallel modes) ----
 template <typename R, int DIM>
 static void cell_d(int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt, const DevWork<R> &wk,
-                   const Gas &gas, double cfl, double dtu, double alpha, int first, int ks, int it, const CellRange &rg,
-                   cudaStream_t s) {
-    const int bs = g.blk_cell, nb = nblocks(rg.c1 - rg.c0, bs);
-    if (nb == 0) return;
+                   const Gas &gas, double cfl, double dtu, double alpha, int first, int ks, int it, cudaStream_t s) {
+    const int bs = g.blk_cell, nb = nblocks(g.nint, bs);
     if (g.cell_case) {  // merged grids: per-case run flags and residual columns
         if (lc == 1)
-            k_cell<R, DIM, 1, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+            k_cell<R, DIM, 1, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         else if (lc == 2)
-            k_cell<R, DIM, 2, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+            k_cell<R, DIM, 2, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         else
-            k_cell<R, DIM, 0, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+            k_cell<R, DIM, 0, true><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
         return;
     }
     if (lc == 1)
-        k_cell<R, DIM, 1, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+        k_cell<R, DIM, 1, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
     else if (lc == 2)
-        k_cell<R, DIM, 2, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+        k_cell<R, DIM, 2, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
     else
-        k_cell<R, DIM, 0, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it, rg);
+        k_cell<R, DIM, 0, false><<<nb, bs, 0, s>>>(g, cur, nxt, wk, gas, cfl, dtu, alpha, first, ks, it);
 }
 
 template <typename R>
 void Ops<R>::cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, const DevState<R> &nxt,
                   const DevWork<R> &wk, const Gas &gas, double cfl, double dt_uniform, double alpha, int stage,
-                  int kstage, int it_slot, cudaStream_t s, const CellRange *range) {
+                  int kstage, int it_slot, cudaStream_t s) {
     if (g.nint == 0) return;
-    // a range starts on a multiple of 256 cells, so blk0 is whole for every launch shape
-    const CellRange all{0, g.nint, 0, nblocks(g.nint, g.blk_cell)};
-    CellRange rg = range ? *range : all;
-    rg.blk0 = rg.c0 / g.blk_cell;
-    rg.nblk = nblocks(g.nint, g.blk_cell);
     if (dim == 2)
-        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, rg, s);
+        cell_d<R, 2>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, s);
     else
-        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, rg, s);
+        cell_d<R, 3>(lc, g, cur, nxt, wk, gas, cfl, dt_uniform, alpha, stage, kstage, it_slot, s);
 }
 
 template <typename R>

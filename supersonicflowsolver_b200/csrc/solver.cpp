@@ -455,13 +455,6 @@ struct psst_solver {
     // sequential LocalAccTime1 as one persistent launch per call (FP64, single
     // grids): schedule uploaded (wf_ready), switched on (wf_on), CTAs, and the
     // bound of every grid-barrier wait
-    // face/cell chunk interleave of the parallel modes: chunk k's faces (those
-    // whose lower cell is in cell chunk k) then chunk k's cells, so the cell
-    // pass finds the chunk's face outputs in L2. chunks_req: 0 automatic, 1
-    // off, n > 1 n chunks; fr/cr: the ranges in use (empty: no interleave)
-    int chunks_req = 0;
-    std::vector<FaceRange> fr;
-    std::vector<CellRange> cr;
     // merged grids: the per-case stop rule evaluated on the device (CaseStop)
     bool stop_on = false;
     CaseStop stop{};
@@ -640,39 +633,6 @@ void check_err(psst_solver *s, const int32_t *err_dev) {
 
 enum Kind { K_GRADIENT = 0, K_FACE = 1, K_CELL = 2, K_GHOST = 3, K_NORM = 4 };
 
-// Chunk ranges of the face/cell interleave for `chunks` chunks (<= 1: none).
-// Cell chunks start on multiples of 256 cells; face chunk k holds the faces
-// whose lower cell is in cell chunk k (faces are sorted by lower cell, interior
-// faces first, then boundary faces), so cell chunk k needs face chunks <= k.
-void set_chunks(psst_solver *s, int chunks) {
-    s->fr.clear();
-    s->cr.clear();
-    const Layout &L = s->L;
-    if (chunks <= 1 || L.nint < 2 * 256) return;
-    const int64_t units = (L.nint + 255) / 256;
-    chunks = (int)std::min<int64_t>(chunks, units);
-    auto low = [&](int32_t f) { return std::min(L.c0[f], L.c1[f]); };
-    int32_t fi = 0, fb = L.nfi;
-    for (int k = 0; k < chunks; ++k) {
-        const int32_t c0 = (int32_t)(units * k / chunks * 256);
-        const int32_t c1 = k + 1 == chunks ? L.nint : (int32_t)(units * (k + 1) / chunks * 256);
-        int32_t fi1 = fi, fb1 = fb;
-        while (fi1 < L.nfi && low(fi1) < c1) ++fi1;
-        while (fb1 < L.nface && low(fb1) < c1) ++fb1;
-        s->fr.push_back(FaceRange{fi, fi1 - fi, fb, fb1 - fb, 1});
-        s->cr.push_back(CellRange{c0, c1, 0, 0});
-        fi = fi1;
-        fb = fb1;
-    }
-}
-
-// The automatic chunk count: none while the face outputs fit in about half of
-// the 126 MB L2; otherwise chunks of about 48 MB of face outputs.
-int auto_chunks(const psst_solver *s, size_t fout_bytes) {
-    const double bytes = (double)s->L.nface * (double)fout_bytes;
-    return bytes <= 64e6 ? 1 : (int)std::ceil(bytes / 48e6);
-}
-
 // One RK stage. The parallel modes run face pass -> cell pass (the cell pass
 // also updates ghosts and finishes the norms); the sequential LocalAccTime1
 // mode and the stage-by-stage API (gather == false: residual already in
@@ -683,23 +643,6 @@ void one_stage(psst_solver *s, int k, int it_slot, bool gather, Mark &&mark) {
     DevState<R> *st = states<R>(s);
     DevWork<R> &w = work<R>(s);
     const DevState<R> &cur = st[s->cur], &nxt = st[s->cur ^ 1];
-    if (gather && !s->seq && !s->fr.empty()) {  // face/cell chunk interleave
-        const int stage = (k == 0 ? 1 : 0) | (k == s->sc.rk_level - 1 ? 2 : 0);
-        for (size_t q = 0; q < s->fr.size(); ++q) {
-            Ops<R>::face(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->sc.lc, s->g, cur, w, s->gas, s->stream,
-                         &s->fr[q]);
-            mark(K_FACE);
-            Ops<R>::cell(s->dim, s->sc.lc, s->g, cur, nxt, w, s->gas, s->sc.cfl, s->dt_uniform, s->sc.rk[k], stage,
-                         k, it_slot, s->stream, &s->cr[q]);
-            mark(K_CELL);
-        }
-        if (k == s->sc.rk_level - 1) {  // the iteration's residual columns
-            Ops<R>::norm_reduce(s->dim, s->g, w, s->sc.rk_level, it_slot, s->stream);
-            mark(K_NORM);
-        }
-        s->cur ^= 1;
-        return;
-    }
     if (gather) {
         Ops<R>::face(s->dim, s->sc.flux, s->rec, s->sc.limiter, s->seq ? 0 : s->sc.lc, s->g, cur, w, s->gas,
                      s->stream);
@@ -1259,8 +1202,6 @@ extern "C" psst_status psst_solver_create(const psst_grid *G, const psst_scheme 
         alloc_state<float>(s.get(), *G);
     else
         alloc_state<double>(s.get(), *G);
-    set_chunks(s.get(), auto_chunks(s.get(), sc->precision == 32 ? Ops<float>::face_out_bytes(s->dim)
-                                                                   : Ops<double>::face_out_bytes(s->dim)));
     if (s->seq && sc->precision == 64 && L.cell_case.empty() && !L.wf_item_level.empty()) {
         const int maxb = Ops<double>::wavefront_max_blocks(s->dim, s->rec, sc->limiter);
         // CTA 0 folds the norms; the others take the work items of a step
@@ -1549,18 +1490,6 @@ extern "C" psst_status psst_solver_case_residuals(psst_solver *s, int n_iter, do
        "norm copy");
     ck(cudaStreamSynchronize(s->stream), "stream sync");
     for (size_t i = 0; i < cnt; ++i) std::memcpy(out + i, &h[i], sizeof(double));
-    PSST_API_END
-}
-
-extern "C" psst_status psst_solver_set_chunks(psst_solver *s, int chunks, int *in_use) {
-    PSST_API_BEGIN
-    if (!s) raise(PSST_ERR_ARG, "null solver");
-    if (chunks < 0) raise(PSST_ERR_ARG, "chunks must be >= 0");
-    s->drop_graphs();
-    s->chunks_req = chunks;
-    const size_t fo = s->sc.precision == 32 ? Ops<float>::face_out_bytes(s->dim) : Ops<double>::face_out_bytes(s->dim);
-    set_chunks(s, chunks == 0 ? auto_chunks(s, fo) : chunks);
-    if (in_use) *in_use = s->fr.empty() ? 1 : (int)s->fr.size();
     PSST_API_END
 }
 

@@ -267,13 +267,6 @@ class Solver:
 
     graphs_on = False
 
-    def set_chunks(self, chunks=0):
-        """Face/cell chunk interleave (0 automatic, 1 off, n chunks); returns
-        the chunk count in use."""
-        n = ctypes.c_int()
-        check(_lib.load().psst_solver_set_chunks(self._h, int(chunks), ctypes.byref(n)))
-        return n.value
-
     def use_wavefront(self, on=True):
         """Sequential LocalAccTime1 as one persistent launch per call (default
         on) or level by level, stage by stage (off); same results."""

@@ -219,18 +219,3 @@ def test_unconverged_summary_bins_every_case():
     assert tot == 64 and ok == sum(i is not None for i in its)
     assert sum(int(v.split("/")[1]) for v in w["by_mesh"].values()) == 64
     assert {c["index"] for c in w["unconverged"]} == {i for i, x in enumerate(its) if x is None}
-
-
-@pytest.mark.gpu
-def test_merged_grid_chunks_keep_results(tmp_path):
-    """The face/cell chunk interleave on a merged grid (chunk boundaries cut
-    through cases): the same states and per-case residual columns."""
-    grids, schemes, prims, m = build(tmp_path)
-    outs = []
-    for chunks in (1, 4):
-        b = Solver(m, schemes[0])
-        assert b.set_chunks(chunks) == chunks
-        b.set_state(m.initial_state())
-        b.explicit_solve(4)
-        outs.append((b.get_state(), b.case_residuals(4)))
-    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])

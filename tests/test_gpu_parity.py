@@ -345,23 +345,3 @@ def test_fp64_bit_exact_on_48k_tets(tmp_path, lc1_mode, n):
         assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim)), "state, iteration %d" % (it + 1)
     for k in ("grad_p", "grad_T", "grad_u"):
         assert np.array_equal(s.get(k).reshape(g.nvol, -1)[interior], o.get("vol_l" + k).reshape(g.nvol, -1)[interior])
-
-
-@pytest.mark.parametrize("precision,lc,mesh", [(64, 1, "3d"), (32, 2, "2d"), (32, 1, "3d")],
-                         ids=["fp64_lc1_tets", "fp32_lc2_quads", "fp32_lc1_tets"])
-def test_face_cell_chunks_keep_results(tmp_path, precision, lc, mesh):
-    """The face/cell chunk interleave (chunk k's faces, then chunk k's cells)
-    gives the same state, residual columns and RMS column bit for bit as the
-    whole-mesh passes."""
-    m = meshgen.wedge3d(12, 6, 4, 12.0, tets=True) if mesh == "3d" else meshgen.wedge2d(60, 20, 15.0, jitter=0.1)
-    path, d, name = make_case(tmp_path, m, max_iter=5, flux=3, order=2, limiter=5, lc=lc,
-                              mach=3.0 if m.dim == 3 else 2.5)
-    runs = []
-    for chunks in (1, 3, 7):
-        g, s = gpu_solver(path, d, name, precision=precision, lc1_mode=1)
-        assert s.set_chunks(chunks) == min(chunks, -(-g.ninterior // 256))
-        linf, l2 = s.explicit_solve(5)
-        runs.append((s.get_state(), linf, l2))
-    for r in runs[1:]:
-        for a, b in zip(runs[0], r):
-            assert np.array_equal(a, b)
