@@ -49,7 +49,7 @@ static bool write_sav(const char *path, const psst_grid_info &gi, const std::vec
 }
 
 int main(int argc, char **argv) {
-    int precision = 64, jacobi = 0, renumber = 1, device = 0, chunk = 100;
+    int precision = 64, jacobi = 0, renumber = 1, device = 0, chunk = 1000;
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--precision") && i + 1 < argc)
             precision = std::atoi(argv[++i]);
