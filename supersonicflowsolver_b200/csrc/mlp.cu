@@ -531,7 +531,15 @@ constexpr size_t kGemmSmem = 100 * 1024;  // at most two CTAs per SM, so two 256
 
 template <int NT>
 void gemm(const GemmArgs &a, int splits, cudaStream_t s) {
-    ck(cudaFuncSetAttribute(k_gemm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem), "attribute");
+    // once per device (a per-launch call costs host time between back-to-back GEMMs)
+    static thread_local unsigned long long done_devices = 0;
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev >= 64 || !(done_devices >> dev & 1ull)) {
+        ck(cudaFuncSetAttribute(k_gemm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem),
+           "attribute");
+        if (dev < 64) done_devices |= 1ull << dev;
+    }
     dim3 grid((a.M + kTileM - 1) / kTileM, (a.N + NT - 1) / NT, splits);
     k_gemm<NT><<<grid, kThreads, kGemmSmem, s>>>(a);
 }
