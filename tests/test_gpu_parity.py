@@ -345,3 +345,26 @@ def test_fp64_bit_exact_on_48k_tets(tmp_path, lc1_mode, n):
         assert np.array_equal(s.get_state(), oracle_prim(o, g.nvol, g.dim)), "state, iteration %d" % (it + 1)
     for k in ("grad_p", "grad_T", "grad_u"):
         assert np.array_equal(s.get(k).reshape(g.nvol, -1)[interior], o.get("vol_l" + k).reshape(g.nvol, -1)[interior])
+
+
+def test_fp32_converged_field_close_to_fp64(tmp_path):
+    """At convergence (first order, HLL, 60 x 20 quads, 2500 iterations: the
+    residual drops by more than 1e-4 on both paths) the FP32 production path's
+    density, pressure and Mach number stay within 1e-4 relative of the FP64
+    path (bit-exact with the oracle), cell by cell."""
+    m = meshgen.wedge2d(60, 20, 10.0)
+    path, d, name = make_case(tmp_path, m, max_iter=2500, flux=2, order=1, lc=1, rk_level=1, cfl=0.8, mach=2.5)
+    fields = []
+    for precision in (64, 32):
+        g, s = gpu_solver(path, d, name, precision=precision, lc1_mode=1)
+        linf, _ = s.explicit_solve(2500)
+        assert np.all(linf[-1] <= 1e-4 * linf[:5].max(axis=0) + 1e-300)
+        prim = s.get_state()
+        nv = g.nvol
+        T = prim[nv:2 * nv]
+        speed = np.hypot(prim[2 * nv:3 * nv], prim[3 * nv:])
+        fields.append((s.get("rho"), prim[:nv], speed / np.sqrt(1.4 * 287.0 * T)))
+    interior = g.get("vol_bc") == 1
+    for a, b in zip(fields[1], fields[0]):
+        rel = np.abs(a[interior] - b[interior]) / np.abs(b[interior])
+        assert rel.max() < 1e-4, rel.max()
