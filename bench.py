@@ -424,9 +424,11 @@ def gemm_throughput():
     FP32) on the warm-start network's training shapes: a hidden layer forward
     (16384 points x 256 outputs x 256 inputs, both operands contiguous along
     K) and its weight gradient (256 x 256 over 16384 points, both operands
-    contiguous along M/N, split over K in 256-row slices). TFLOP/s against
-    the measured BF16 peak and against each shape's own HBM bound (operands
-    read once, FP32 result written once)."""
+    contiguous along M/N, split over K in 256-row slices), plus a square
+    8192^3 product that the tensor cores bound. TFLOP/s against the measured
+    BF16 peak and against each shape's own HBM bound (operands read once,
+    FP32 result written once); device time per launch, launches back to
+    back."""
     import torch
     from supersonicflowsolver_b200.mlp import tc_gemm_time
 
@@ -439,12 +441,15 @@ def gemm_throughput():
     W = torch.randn((256, 256), generator=g, device="cuda").to(torch.bfloat16)
     Y = torch.randn((16384, 256), generator=g, device="cuda").to(torch.bfloat16)
     out = {"peak_tflops": peak, "peak_kind": peak_kind}
-    for name, kw, M, N, K, dbytes in (
-            ("forward_16384x256x256", dict(A=X, B=W), 16384, 256, 256, 16384 * 256 * 4),
+    S = torch.randn((8192, 8192), generator=g, device="cuda").to(torch.bfloat16)
+    T = torch.randn((8192, 8192), generator=g, device="cuda").to(torch.bfloat16)
+    for name, kw, M, N, K, dbytes, reps in (
+            ("forward_16384x256x256", dict(A=X, B=W), 16384, 256, 256, 16384 * 256 * 4, 20),
             ("weight_grad_256x256x16384", dict(A=X, B=Y, a_strides=(1, 256), b_strides=(1, 256), M=256, N=256,
-                                               K=16384, k_split=256), 256, 256, 16384, 64 * 256 * 256 * 4)):
-        tc_gemm_time(reps=3, **kw)
-        ms = tc_gemm_time(reps=20, **kw)
+                                               K=16384, k_split=256), 256, 256, 16384, 64 * 256 * 256 * 4, 20),
+            ("square_8192", dict(A=S, B=T), 8192, 8192, 8192, 8192 * 8192 * 4, 5)):
+        tc_gemm_time(reps=2, **kw)
+        ms = tc_gemm_time(reps=reps, **kw)
         flops = 2.0 * M * N * K
         byts = 2.0 * (M * K + N * K) + dbytes
         tf = flops / (ms * 1e-3) / 1e12
@@ -630,9 +635,14 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the FP64 line and the FP32-vs-FP64 field error of the 6M-tet workload")
+    ap.add_argument("--gemm-only", action="store_true",
+                    help="print only the tensor-core GEMM figures (the tensor_gemm object) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    if args.gemm_only:
+        print(json.dumps({"tensor_gemm": gemm_throughput()}))
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

@@ -10,20 +10,29 @@
 //   y  = W6 h5 + b6                                  (4 outputs: rho, u, v, p)
 // Loss: mean over points and outputs of (y - target)^2.
 //
-// GEMM kernel: one CTA computes a 128 x NT tile of D = A . B^T, A [M x K],
+// GEMM kernels: one CTA computes a 128 x NT tile of D = A . B^T, A [M x K],
 // B [N x K] given by element strides (so transposed operands need no copy).
-// K is walked in 64-wide chunks through two shared-memory stages in the UMMA
-// K-major no-swizzle layout (8-row x 16-byte core matrices): while the tensor
-// core runs the four tcgen05.mma.kind::f16 (M = 128, N = NT, K = 16) of chunk
-// k, issued by one thread and committed to that stage's mbarrier, the CTA
-// stages chunk k+1 into the other stage. Operands contiguous along K load as
-// 16-byte vectors; operands contiguous along M/N (the transposed ones) load as
-// 16-byte vectors along M/N and are transposed in registers, 8 x 8 at a time.
-// The epilogue reads the accumulator with tcgen05.ld (one row per thread),
-// applies bias / SiLU / SiLU-derivative, and writes through a per-warp
-// shared-memory tile so that global stores are row-contiguous. Split-K over
-// gridDim.z writes FP32 partials that a second kernel sums in a fixed order
-// (deterministic). Every mbarrier wait is bounded.
+// K is walked in 64-wide chunks, four tcgen05.mma.kind::f16 (M = 128, N = NT,
+// K = 16) per chunk, issued by one thread, FP32 accumulators in tensor memory.
+//  * k_gemm_tma (operands 16-byte aligned with 16-byte row strides, contiguous
+//    along K or along M/N): TMA tile loads (cp.async.bulk.tensor, no
+//    multicast) into four shared-memory stages in the 128-byte swizzled
+//    layout, each stage's mbarrier completed by the copy's byte count; the
+//    issuing thread keeps up to four chunks in flight and refills the stage of
+//    chunk c - 1 once the MMAs committed for it have completed. Operands
+//    contiguous along M/N are loaded as such and read by the MMA in its
+//    MN-major mode.
+//  * k_gemm (anything else: unaligned strides, element strides on both axes,
+//    split ranges that are not whole chunks): the CTA stages each chunk
+//    through registers into the K-major no-swizzle layout (8-row x 16-byte
+//    core matrices), two stages, transposing operands contiguous along M/N in
+//    registers, 8 x 8 at a time.
+// The epilogue reads the accumulator with tcgen05.ld (one row per thread, 32
+// columns at a time), applies bias / SiLU / SiLU-derivative and writes each
+// row segment with 16-byte stores. Split-K over gridDim.z writes FP32
+// partials that a second kernel sums in a fixed order (deterministic). Every
+// mbarrier wait is bounded; a wait that runs out drains the MMAs and copies in
+// flight before the CTA frees its tensor memory and reports the timeout.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -31,6 +40,7 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched through the runtime)
 #include <cuda_bf16.h>
 #include <cuda_runtime_api.h>
 
@@ -59,10 +69,21 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major, M = 128.
-template <int NT>
+// The same for the 128-byte swizzled layouts written by TMA (tiles 1024-byte
+// aligned, layout type 2): K-major, 8-row groups of 128-byte rows 1024 bytes
+// apart (SBO), LBO unused (16); MN-major, groups of 8 K rows 1024 bytes apart
+// (SBO) and 64-element M/N blocks `lbo` bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr, uint32_t lbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, M = 128; operand A (B) read
+// K-major, or MN-major when AMN (BMN).
+template <int NT, bool AMN = false, bool BMN = false>
 __device__ __forceinline__ uint32_t umma_idesc() {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)AMN << 15) | ((uint32_t)BMN << 16) |
+           ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
@@ -86,14 +107,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, unsigne
     return false;
 }
 
-template <int NT>
+template <int NT, bool AMN = false, bool BMN = false>
 __device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
-    const uint32_t idesc = umma_idesc<NT>();
+    const uint32_t idesc = umma_idesc<NT, AMN, BMN>();
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
         "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// One TMA tile load (no multicast) of the box at coordinates (x, y) of `map`;
+// completes its bytes on `bar`.
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -138,7 +174,141 @@ struct GemmArgs {
     int64_t d_sm;
     int *err;
     unsigned wait_polls;  // bound of the first wait that runs out (kWaitLimit; 0 gives up at once)
+    int vec;              // outputs and Zin 16-byte aligned, d_sm % 8 == 0: 16-byte epilogue stores
 };
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+constexpr int kEpiWarpBytes = 8192;  // per warp: a 32 x 32 FP32 tile (4 KB) + two BF16 tiles (2 KB each)
+
+// Swizzled 32-row tiles in shared memory: 16-byte chunk c of row r of an FP32
+// tile (128-byte rows) at r * 128 + (c ^ (r & 7)) * 16, of a BF16 tile
+// (64-byte rows) at r * 64 + (c ^ ((r >> 1) & 3)) * 16. A warp writing one
+// row per lane, or reading 512 contiguous bytes, hits every bank 4 times.
+__device__ __forceinline__ uint4 *tile32(unsigned char *t, int r, int c) {
+    return reinterpret_cast<uint4 *>(t + r * 128 + ((c ^ (r & 7)) << 4));
+}
+__device__ __forceinline__ uint4 *tile16(unsigned char *t, int r, int c) {
+    return reinterpret_cast<uint4 *>(t + r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
+}
+
+// Writes the warp's BF16 tile (rows m0w.., columns nb..nb+31) to g (row
+// stride ld): each store instruction covers 8 rows x 64 bytes.
+__device__ __forceinline__ void tile16_store(unsigned char *t, bf16 *g, int64_t ld, int m0w, int M, int nb) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = 8 * i + (lane >> 2), c = lane & 3;
+        if (m0w + r < M) *reinterpret_cast<uint4 *>(g + (int64_t)(m0w + r) * ld + nb + 8 * c) = *tile16(t, r, c);
+    }
+    __syncwarp();
+}
+
+// Epilogue: thread t holds accumulator row m0 + t (TMEM lane t) and handles it
+// 32 columns at a time: bias and activation in registers; then, with a.vec and
+// the whole segment inside N, each warp passes its 32 x 32 block through its
+// shared-memory tiles so that global loads and stores cover whole rows (16
+// bytes per lane); otherwise element by element. `tiles`: kEpiWarpBytes per
+// warp of free shared memory.
+template <int NT>
+__device__ __forceinline__ void epilogue(const GemmArgs &a, uint32_t tmem, int m0, int n0, bool empty,
+                                         unsigned char *tiles) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m0w = m0 + 32 * warp, m = m0w + lane;
+    const uint32_t lanes = (uint32_t)(32 * warp) << 16;  // this warp's 32 TMEM lanes
+    unsigned char *tf = tiles + warp * kEpiWarpBytes, *th = tf + 4096, *tz = th + 2048;
+    for (int c0 = 0; c0 < NT && n0 + c0 < a.N; c0 += 32) {
+        float v[32];
+        if (!empty)
+            tmem_ld32(tmem + lanes + (uint32_t)c0, v);
+        else
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = 0.0f;
+        const int nb = n0 + c0, nn = min(32, a.N - nb);
+        if (a.bias)
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                if (i < nn) v[i] += a.bias[nb + i];
+        if (a.vec && nn == 32) {  // warp-uniform
+            if (a.D32) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    *tile32(tf, lane, j) = make_uint4(__float_as_uint(v[4 * j]), __float_as_uint(v[4 * j + 1]),
+                                                      __float_as_uint(v[4 * j + 2]), __float_as_uint(v[4 * j + 3]));
+                __syncwarp();
+                float *d32 = a.D32 + (int64_t)blockIdx.z * a.M * a.d_sm;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {  // 4 rows x 128 bytes per instruction
+                    const int r = 4 * i + (lane >> 3), c = lane & 7;
+                    if (m0w + r < a.M)
+                        *reinterpret_cast<uint4 *>(d32 + (int64_t)(m0w + r) * a.d_sm + nb + 4 * c) = *tile32(tf, r, c);
+                }
+                __syncwarp();
+            }
+            if (a.epi == EPI_SILU && a.Z16) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    *tile16(tz, lane, j) =
+                        make_uint4(pack_bf16(v[8 * j], v[8 * j + 1]), pack_bf16(v[8 * j + 2], v[8 * j + 3]),
+                                   pack_bf16(v[8 * j + 4], v[8 * j + 5]), pack_bf16(v[8 * j + 6], v[8 * j + 7]));
+                tile16_store(tz, a.Z16, a.d_sm, m0w, a.M, nb);
+            }
+            if (a.D16) {
+                if (a.epi == EPI_SILU) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = silu(v[i]);
+                } else if (a.epi == EPI_DSILU) {
+                    // the pre-activations of the warp's rows, loaded whole rows at a time
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int r = 8 * i + (lane >> 2), c = lane & 3;
+                        if (m0w + r < a.M)
+                            *tile16(tz, r, c) =
+                                *reinterpret_cast<const uint4 *>(a.Zin + (int64_t)(m0w + r) * a.d_sm + nb + 8 * c);
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const uint4 zq = *tile16(tz, lane, j);
+                        const uint32_t zw[4] = {zq.x, zq.y, zq.z, zq.w};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const __nv_bfloat162 z2 = *reinterpret_cast<const __nv_bfloat162 *>(&zw[q]);
+                            v[8 * j + 2 * q] *= dsilu(__low2float(z2));
+                            v[8 * j + 2 * q + 1] *= dsilu(__high2float(z2));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    *tile16(th, lane, j) =
+                        make_uint4(pack_bf16(v[8 * j], v[8 * j + 1]), pack_bf16(v[8 * j + 2], v[8 * j + 3]),
+                                   pack_bf16(v[8 * j + 4], v[8 * j + 5]), pack_bf16(v[8 * j + 6], v[8 * j + 7]));
+                tile16_store(th, a.D16, a.d_sm, m0w, a.M, nb);
+            }
+        } else if (m < a.M) {
+            const int64_t o = (int64_t)m * a.d_sm + nb;
+            float *d32 = a.D32 ? a.D32 + (int64_t)blockIdx.z * a.M * a.d_sm + o : nullptr;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {  // unrolled: v stays in registers
+                if (i >= nn) break;
+                const float z = v[i];
+                if (d32) d32[i] = z;
+                if (a.epi == EPI_SILU && a.Z16) a.Z16[o + i] = __float2bfloat16(z);
+                if (a.D16) {
+                    float h = z;
+                    if (a.epi == EPI_SILU) h = silu(z);
+                    else if (a.epi == EPI_DSILU) h = z * dsilu(__bfloat162float(a.Zin[o + i]));
+                    a.D16[o + i] = __float2bfloat16(h);
+                }
+            }
+        }
+    }
+}
 
 // Stages rows [r0, r0+ROWS) x K columns [k0, k0+64) of a strided BF16 matrix
 // (element (r, k) at g[r * sr + k * sk]) into the K-major no-swizzle layout:
@@ -237,7 +407,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm(GemmArgs a) {
     __shared__ int failed;
     const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * NT;
     const int kb = blockIdx.z * a.k_split, ke = min(a.K, kb + a.k_split);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                      "r"(NT < 32 ? 32 : NT));
@@ -299,60 +469,120 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm(GemmArgs a) {
     if (failed) {
         if (threadIdx.x == 0) atomicExch(a.err, MLP_ERR_TIMEOUT);
     } else {
-        // epilogue: thread t holds row m0 + t (TMEM lane t); each warp writes its
-        // 32 rows x 32 columns at a time through its own shared tile, a row per
-        // store instruction (the operand stages are free now)
-        float *tf = reinterpret_cast<float *>(smem) + warp * 32 * 33;
-        bf16 *th = reinterpret_cast<bf16 *>(smem + 4 * 32 * 33 * 4) + warp * 32 * 34;
-        bf16 *tz = reinterpret_cast<bf16 *>(smem + 4 * 32 * 33 * 4 + 4 * 32 * 34 * 2) + warp * 32 * 34;
-        const int rw = warp * 32;  // first row of this warp in the tile
-        const bool empty = nchunks == 0;
-        for (int c0 = 0; c0 < NT && n0 + c0 < a.N; c0 += 32) {
-            float v[32];
-            if (!empty)
-                tmem_ld32(tmem + ((uint32_t)rw << 16) + (uint32_t)c0, v);
-            else
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = 0.0f;
-            const int nn = n0 + c0 + lane;  // column this lane stores
-            if (a.epi == EPI_DSILU) {        // the pre-activations of these rows, loaded row by row
-                for (int r = 0; r < 32; ++r) {
-                    const int m = m0 + rw + r;
-                    if (m < a.M && nn < a.N) tz[r * 34 + lane] = a.Zin[(int64_t)m * a.d_sm + nn];
-                }
-                __syncwarp();
-            }
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int n = n0 + c0 + i;
-                float z = v[i];
-                if (a.bias && n < a.N) z += a.bias[n];
-                tf[lane * 33 + i] = z;
-                if (a.epi == EPI_SILU) {
-                    th[lane * 34 + i] = __float2bfloat16(silu(z));
-                } else if (a.epi == EPI_DSILU) {
-                    th[lane * 34 + i] = __float2bfloat16(z * dsilu(__bfloat162float(tz[lane * 34 + i])));
-                } else {
-                    th[lane * 34 + i] = __float2bfloat16(z);
-                }
-            }
-            __syncwarp();
-            for (int r = 0; r < 32; ++r) {
-                const int m = m0 + rw + r;
-                if (m >= a.M || nn >= a.N) continue;
-                const int64_t o = (int64_t)m * a.d_sm + nn;
-                const float z = tf[r * 33 + lane];
-                if (a.D32) a.D32[(int64_t)blockIdx.z * a.M * a.d_sm + o] = z;
-                if (a.epi == EPI_SILU && a.Z16) a.Z16[o] = __float2bfloat16(z);
-                if (a.D16) a.D16[o] = th[r * 34 + lane];
-            }
-            __syncwarp();
-        }
+        epilogue<NT>(a, tmem, m0, n0, nchunks == 0, smem);  // the operand stages are free now
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT < 32 ? 32 : NT));
+}
+
+constexpr int kTmaStages = 4;  // chunks in flight: K = 256 (the network's widths) loads in one go
+
+// TMA-fed variant. Stage s holds the A tile then the B tile of one 64-wide K
+// chunk in the 128-byte swizzled layout: K-major operands as one box of
+// (64 k) x rows, rows 128 bytes apart; MN-major operands as boxes of
+// (64 rows) x (64 k), one per 64 rows, K rows 128 bytes apart. Thread 0
+// issues the copies and the MMAs: the first kTmaStages chunks are loaded at
+// once; after the MMAs of chunk c are issued, the stage of chunk c - 1 is
+// refilled (with chunk c - 1 + kTmaStages) as soon as its MMAs have completed.
+template <int NT, bool AMN, bool BMN>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs a) {
+    constexpr uint32_t kABytes = kTileM * kChunkK * 2, kBBytes = NT * kChunkK * 2, kStage = kABytes + kBBytes;
+    extern __shared__ unsigned char smem_raw[];
+    // the swizzle pattern repeats every 1024 bytes: tiles start on that boundary
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * NT;
+    const int kb = blockIdx.z * a.k_split, ke = min(a.K, kb + a.k_split);
+    const int nchunks = ke > kb ? (ke - kb + kChunkK - 1) / kChunkK : 0;
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(NT));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < kTmaStages; ++b) {
+            mbar_init(&full[b], 1);
+            mbar_init(&empty[b], 1);
+        }
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    if (threadIdx.x == 0) {
+        const unsigned polls = a.wait_polls;  // 0: the first wait gives up at once
+        int issued = 0, consumed = 0, committed = 0;
+        auto load = [&](int c) {
+            const int b = c % kTmaStages, k0 = kb + c * kChunkK;
+            unsigned char *sa = smem + b * kStage, *sb = sa + kABytes;
+            mbar_expect_tx(&full[b], kStage);  // out-of-range box elements arrive as zeros and count
+            if (AMN) {
+#pragma unroll
+                for (int j = 0; j < kTileM / 64; ++j) tma_load(sa + j * 8192, &ta, m0 + 64 * j, k0, &full[b]);
+            } else {
+                tma_load(sa, &ta, k0, m0, &full[b]);
+            }
+            if (BMN) {
+#pragma unroll
+                for (int j = 0; j < NT / 64; ++j) tma_load(sb + j * 8192, &tb, n0 + 64 * j, k0, &full[b]);
+            } else {
+                tma_load(sb, &tb, k0, n0, &full[b]);
+            }
+            ++issued;
+        };
+        // use: how many earlier chunks went through this stage (the phase parity to wait for)
+        auto wait = [&](uint64_t *bar, int use) { return polls != 0 && mbar_wait(bar, (unsigned)use & 1u, polls); };
+        bool ok = true;
+        for (int c = 0; c < min(kTmaStages, nchunks); ++c) load(c);
+        for (int c = 0; c < nchunks; ++c) {
+            const int b = c % kTmaStages;
+            if (!(ok = wait(&full[b], c / kTmaStages))) break;
+            ++consumed;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(smem + b * kStage), sb = sa + kABytes;
+#pragma unroll
+            for (int q = 0; q < kChunkK / 16; ++q) {  // K = 16 per MMA: 32 bytes along a row, or 16 K rows
+                const uint64_t da = AMN ? umma_desc_sw128(sa + q * 2048, 8192) : umma_desc_sw128(sa + q * 32, 16);
+                const uint64_t db = BMN ? umma_desc_sw128(sb + q * 2048, 8192) : umma_desc_sw128(sb + q * 32, 16);
+                umma_bf16<NT, AMN, BMN>(tmem, da, db, (c > 0 || q > 0) ? 1u : 0u);
+            }
+            umma_commit(&empty[b]);
+            ++committed;
+            const int next = c - 1 + kTmaStages;
+            if (c >= 1 && next < nchunks) {
+                if (!(ok = wait(&empty[(c - 1) % kTmaStages], (c - 1) / kTmaStages))) break;
+                load(next);
+            }
+        }
+        // the last commit covers every MMA issued before it
+        if (ok && committed > 0) ok = wait(&empty[(committed - 1) % kTmaStages], (committed - 1) / kTmaStages);
+        if (!ok) {
+            // a wait ran out: let the MMAs and the copies in flight finish (bounded) before the
+            // accumulator and the stages are given up
+            failed = 1;
+            if (committed > 0)
+                mbar_wait(&empty[(committed - 1) % kTmaStages], (unsigned)((committed - 1) / kTmaStages) & 1u);
+            for (int c = consumed; c < issued; ++c) mbar_wait(&full[c % kTmaStages], (unsigned)(c / kTmaStages) & 1u);
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(a.err, MLP_ERR_TIMEOUT);
+    } else {
+        epilogue<NT>(a, tmem, m0, n0, nchunks == 0, smem);  // the stages are free now
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT));
 }
 
 // out[i] = sum over z of part[z][i] (fixed order), optional BF16 copy.
@@ -528,20 +758,126 @@ T *dmalloc(std::vector<void *> &list, size_t n) {
 }
 
 constexpr size_t kGemmSmem = 100 * 1024;  // at most two CTAs per SM, so two 256-column TMEM allocations fit
-
 template <int NT>
-void gemm(const GemmArgs &a, int splits, cudaStream_t s) {
-    // once per device (a per-launch call costs host time between back-to-back GEMMs)
-    static thread_local unsigned long long done_devices = 0;
+constexpr size_t tma_smem() {
+    return (size_t)kTmaStages * (kTileM + NT) * kChunkK * 2 + 1024;  // + the 1024-byte alignment of the tiles
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+    static const EncodeTiled fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    if (!fn) raise(PSST_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return fn;
+}
+
+// An operand (element (r, k) at g[r * sr + k * sk]) that TMA can load:
+// 16-byte aligned, contiguous along K or along the rows, 16-byte row stride.
+bool tma_operand(const bf16 *g, int64_t sr, int64_t sk) {
+    if (((uintptr_t)g & 15) != 0) return false;
+    if (sk == 1) return sr > 0 && sr % 8 == 0;
+    if (sr == 1) return sk > 0 && sk % 8 == 0;
+    return false;
+}
+
+// Its tensor map, boxes landing in the 128-byte swizzled layout: contiguous
+// along K, box (64 k) x box_rows; contiguous along the rows, (64 rows) x (64 k).
+CUtensorMap operand_map(const bf16 *g, int64_t sr, int64_t sk, int nrows, int K, int box_rows) {
+    CUtensorMap map;
+    const bool kmajor = sk == 1;
+    const cuuint64_t dim[2] = {(cuuint64_t)(kmajor ? K : nrows), (cuuint64_t)(kmajor ? nrows : K)};
+    const cuuint64_t stride[1] = {(cuuint64_t)(kmajor ? sr : sk) * 2};
+    const cuuint32_t box[2] = {64, (cuuint32_t)(kmajor ? box_rows : 64)};
+    const cuuint32_t estride[2] = {1, 1};
+    const CUresult r = encode_tiled()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(g), dim, stride,
+                                      box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) raise(PSST_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return map;
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
+// once per device and kernel (a per-launch call costs host time between back-to-back GEMMs)
+template <class F>
+void smem_attribute(F *kernel, size_t bytes, unsigned long long &done_devices) {
     int dev = 0;
     ck(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev >= 64 || !(done_devices >> dev & 1ull)) {
-        ck(cudaFuncSetAttribute(k_gemm<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem),
-           "attribute");
+        ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "attribute");
         if (dev < 64) done_devices |= 1ull << dev;
     }
-    dim3 grid((a.M + kTileM - 1) / kTileM, (a.N + NT - 1) / NT, splits);
-    k_gemm<NT><<<grid, kThreads, kGemmSmem, s>>>(a);
+}
+
+template <int NT, bool AMN, bool BMN>
+void launch_tma(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &a, dim3 grid, cudaStream_t s) {
+    static thread_local unsigned long long done_devices = 0;
+    smem_attribute(k_gemm_tma<NT, AMN, BMN>, tma_smem<NT>(), done_devices);
+    k_gemm_tma<NT, AMN, BMN><<<grid, kThreads, tma_smem<NT>(), s>>>(ta, tb, a);
+}
+
+// One GEMM launch worked out once (kernel, grid, tensor maps), launched any
+// number of times.
+struct GemmPlan {
+    GemmArgs a;
+    dim3 grid;
+    int nt = 256;
+    int kind = 0;  // 0: register-staged; 1 + 2 AMN + BMN: TMA-fed
+    CUtensorMap ta, tb;
+};
+
+template <int NT>
+GemmPlan plan(const GemmArgs &a0, int splits) {
+    GemmPlan p;
+    p.a = a0;
+    GemmArgs &a = p.a;
+    a.vec = a.d_sm % 8 == 0 && aligned16(a.D32) && aligned16(a.D16) && aligned16(a.Z16) && aligned16(a.Zin);
+    p.nt = NT;
+    p.grid = dim3((a.M + kTileM - 1) / kTileM, (a.N + NT - 1) / NT, splits);
+    // TMA boxes are whole 64-wide chunks: a split range must be whole chunks unless it is the only one
+    if (a.K > 0 && (splits == 1 || a.k_split % kChunkK == 0) && tma_operand(a.A, a.a_sm, a.a_sk) &&
+        tma_operand(a.B, a.b_sn, a.b_sk)) {
+        p.ta = operand_map(a.A, a.a_sm, a.a_sk, a.M, a.K, kTileM);
+        p.tb = operand_map(a.B, a.b_sn, a.b_sk, a.N, a.K, NT);
+        p.kind = 1 + 2 * (a.a_sk != 1) + (a.b_sk != 1);
+    }
+    return p;
+}
+
+template <int NT>
+void launch_nt(const GemmPlan &p, cudaStream_t s) {
+    switch (p.kind) {
+        case 1: launch_tma<NT, false, false>(p.ta, p.tb, p.a, p.grid, s); return;
+        case 2: launch_tma<NT, false, true>(p.ta, p.tb, p.a, p.grid, s); return;
+        case 3: launch_tma<NT, true, false>(p.ta, p.tb, p.a, p.grid, s); return;
+        case 4: launch_tma<NT, true, true>(p.ta, p.tb, p.a, p.grid, s); return;
+        default: {
+            static thread_local unsigned long long done_devices = 0;
+            smem_attribute(k_gemm<NT>, kGemmSmem, done_devices);
+            k_gemm<NT><<<p.grid, kThreads, kGemmSmem, s>>>(p.a);
+        }
+    }
+}
+
+void launch(const GemmPlan &p, cudaStream_t s) {
+    if (p.nt == 128)
+        launch_nt<128>(p, s);
+    else
+        launch_nt<256>(p, s);
+}
+
+template <int NT>
+void gemm(const GemmArgs &a, int splits, cudaStream_t s) {
+    launch(plan<NT>(a, splits), s);
 }
 
 GemmArgs gargs(const bf16 *A, int64_t a_sm, int64_t a_sk, const bf16 *B, int64_t b_sn, int64_t b_sk, int M, int N,
@@ -819,8 +1155,8 @@ extern "C" void psst_mlp_destroy(psst_mlp *m) { delete m; }
 
 namespace {
 
-// reps > 1 (timing): the kernel launched reps times back to back between two
-// events; *ms receives the mean device time of one launch.
+// ms != null (timing): *ms receives the mean device time of one launch over
+// reps launches replayed back to back.
 void tc_gemm(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn, int64_t b_sk, int M, int N,
              int K, int k_split, float *D, int64_t d_sm, void *stream, unsigned wait_polls, int reps = 1,
              double *ms = nullptr) {
@@ -842,27 +1178,52 @@ void tc_gemm(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b
     a.d_sm = d_sm;
     a.wait_polls = wait_polls;
     const int splits = K == 0 ? 1 : (K + k_split - 1) / k_split;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (ms) {
-        ck(cudaEventCreate(&e0), "event");
-        ck(cudaEventCreate(&e1), "event");
-        ck(cudaEventRecord(e0, s), "event");
-    }
-    for (int r = 0; r < std::max(reps, 1); ++r) {
-        if (N <= 128)
-            gemm<128>(a, splits, s);
-        else
-            gemm<256>(a, splits, s);
-    }
-    ck(cudaGetLastError(), "gemm launch");
-    if (ms) {
-        ck(cudaEventRecord(e1, s), "event");
-        ck(cudaEventSynchronize(e1), "event");
-        float t = 0.0f;
-        ck(cudaEventElapsedTime(&t, e0, e1), "event");
-        *ms = t / std::max(reps, 1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+    const GemmPlan p = N <= 128 ? plan<128>(a, splits) : plan<256>(a, splits);
+    if (!ms) {
+        launch(p, s);
+        ck(cudaGetLastError(), "gemm launch");
+    } else {
+        // timing: the reps launches captured once as a CUDA graph on a private
+        // stream (ordered after the caller's stream) and replayed between two
+        // events, so the figure is device time with no host time between launches
+        launch(p, s);  // first launch of this kernel (module load, attributes) outside the graph
+        ck(cudaGetLastError(), "gemm launch");
+        cudaStream_t ts = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        auto release = [&] {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (ts) cudaStreamDestroy(ts);
+        };
+        try {
+            ck(cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking), "stream");
+            ck(cudaEventCreate(&e0), "event");
+            ck(cudaEventCreate(&e1), "event");
+            ck(cudaEventRecord(e0, s), "event");
+            ck(cudaStreamWaitEvent(ts, e0, 0), "stream wait");
+            ck(cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal), "capture");
+            for (int r = 0; r < reps; ++r) launch(p, ts);
+            ck(cudaStreamEndCapture(ts, &graph), "capture");
+            ck(cudaGraphInstantiate(&exec, graph, 0), "graph");
+            ck(cudaGraphLaunch(exec, ts), "graph");  // warm replay
+            ck(cudaEventRecord(e0, ts), "event");
+            ck(cudaGraphLaunch(exec, ts), "graph");
+            ck(cudaEventRecord(e1, ts), "event");
+            ck(cudaEventSynchronize(e1), "event");
+            float t = 0.0f;
+            ck(cudaEventElapsedTime(&t, e0, e1), "event");
+            *ms = t / reps;
+            ck(cudaEventRecord(e1, ts), "event");
+            ck(cudaStreamWaitEvent(s, e1, 0), "stream wait");
+        } catch (...) {
+            release();
+            throw;
+        }
+        release();
     }
     int e = 0;
     ck(cudaMemcpyAsync(&e, err, sizeof e, cudaMemcpyDeviceToHost, s), "error word");

@@ -19,8 +19,13 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
 
 
+# TMA-fed kernel: row strides that are multiples of 8 elements and split
+# ranges of whole 64-wide chunks (ragged M, N, K edges arrive as zeros); the
+# register-staged kernel: K = 100 or 300 (row strides of 200 / 600 bytes) and
+# split ranges of 96.
 @pytest.mark.parametrize("M,N,K,k_split", [(128, 256, 64, 64), (300, 256, 128, 128), (77, 128, 200, 200),
-                                           (256, 256, 4096, 1024), (512, 128, 256, 256)])
+                                           (256, 256, 4096, 1024), (512, 128, 256, 256), (96, 200, 100, 100),
+                                           (130, 256, 300, 96), (200, 72, 256, 256)])
 def test_tc_gemm_matches_torch_fp32(M, N, K, k_split):
     from supersonicflowsolver_b200.mlp import tc_gemm
 
@@ -95,11 +100,13 @@ def test_mlp_training_reduces_loss():
     assert np.array_equal(net.params(), net2.params())
 
 
-@pytest.mark.parametrize("M,N,K", [(200, 72, 1000), (256, 256, 4096), (40, 136, 64)])
+@pytest.mark.parametrize("M,N,K", [(200, 72, 1000), (256, 256, 4096), (40, 136, 64), (36, 100, 300), (44, 256, 520)])
 def test_tc_gemm_transposed_ragged(M, N, K):
-    """Operands contiguous along M and N (the weight-gradient form), with row
-    counts that are not multiples of the 8-row load units and a ragged last
-    K chunk: loaded as 16-byte vectors and transposed in registers."""
+    """Operands contiguous along M and N (the weight-gradient form) with a
+    ragged last K chunk: with 16-byte row strides (M, N multiples of 8) TMA
+    loads them as they are and the MMA reads them MN-major; otherwise (36,
+    100, 44) they are loaded as 16-byte vectors where aligned, element by
+    element where not, and transposed in registers."""
     from supersonicflowsolver_b200.mlp import tc_gemm
 
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
