@@ -556,9 +556,97 @@ __global__ void __maxnreg__(PSST_BUDGET(R, PSST_FACE_MAXNREG, 128)) k_face(DevGr
 // Gradient (and cell limiter) of one interior cell c from the state records
 // `rec`, written to out[c]. CG: state loads through L2 only (the persistent
 // wavefront kernel, where other CTAs write the states between its steps).
+// FP32 Green-Gauss gradient (and cell limiter) of interior cell c of a mesh
+// with 4 faces per cell, from the per-entry table g.gcoef: the cell's 4
+// values of each component are one 16-byte load (a warp's load covers whole
+// lines), so only the 4 neighbour states are gathered. Face value
+// own + w (oth - own), w the neighbour's weight; the sum runs over the faces
+// in the cell's CSR order as the general path does.
+template <int DIM, int CELLLIM>
+__device__ __forceinline__ void gradient_cell_table(const DevGrid &g, const CellRec<float> *rec,
+                                                    GradRec<float, DIM> *gout, int32_t c) {
+    constexpr int NVAR = DIM + 2;
+    const int4 nb = *reinterpret_cast<const int4 *>(g.csr_nb + 4 * c);
+    const CellRec<float> r4[4] = {ldg(rec + nb.x), ldg(rec + nb.y), ldg(rec + nb.z), ldg(rec + nb.w)};
+    const Prim<float, DIM> own = unpack<float, DIM>(ldg(rec + c));
+    const float4 *tab = reinterpret_cast<const float4 *>(g.gcoef) + c;  // component j at tab[j * nint]
+    float4 sn[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) sn[k] = tab[(int64_t)k * g.nint];
+    const float4 wn = tab[(int64_t)DIM * g.nint];
+    auto at = [](const float4 &v, int q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; };
+    float gr[NVAR][DIM], mx[NVAR], mn[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) {
+        mx[i] = mn[i] = pvar<float, DIM>(own, i);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) gr[i][k] = 0.0f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const Prim<float, DIM> oth = unpack<float, DIM>(r4[q]);
+        const float w = at(wn, q);
+#pragma unroll
+        for (int i = 0; i < NVAR; ++i) {
+            const float a = pvar<float, DIM>(own, i), o = pvar<float, DIM>(oth, i);
+            if (CELLLIM) {
+                mx[i] = fmaxf(mx[i], o);
+                mn[i] = fminf(mn[i], o);
+            }
+            const float tv = fmaf(w, o - a, a);
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) gr[i][k] = fmaf(tv, at(sn[k], q), gr[i][k]);
+        }
+    }
+    float lim[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) lim[i] = 1.0f;
+    if (CELLLIM) {
+        float4 off[DIM];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) off[k] = tab[(int64_t)(DIM + 1 + k) * g.nint];
+        const float eps2 = CELLLIM == 5 ? (float)g.vk_eps2[c] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i) {
+                const float phic = pvar<float, DIM>(own, i);
+                float dm = 0.0f;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) dm += gr[i][k] * at(off[k], q);
+                float pf = 1.0f;
+                if (dm != 0.0f) {
+                    const float dp = dm > 0.0f ? mx[i] - phic : mn[i] - phic;
+                    if (CELLLIM == 4) {
+                        const float y = __fdividef(dp, dm);
+                        pf = y < 1.0f ? y : 1.0f;
+                    } else {
+                        const float num = (dp * dp + eps2) + 2.0f * dm * dp;
+                        const float den = dp * dp + 2.0f * dm * dm + dm * dp + eps2;
+                        pf = __fdividef(num, den);
+                    }
+                }
+                if (pf < lim[i]) lim[i] = pf;
+            }
+        }
+    }
+    GradRec<float, DIM> out;
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = CELLLIM ? gr[i][k] * lim[i] : gr[i][k];
+    st16(gout + c, out);
+}
+
 template <typename R, int DIM, int GRAD, int CELLLIM, bool CG>
 __device__ __forceinline__ void gradient_cell(const DevGrid &g, const CellRec<R> *rec, GradRec<R, DIM> *gout,
                                               int32_t c) {
+    if constexpr (sizeof(R) == 4 && GRAD == 1 && !CG) {
+        if (g.gcoef) {
+            gradient_cell_table<DIM, CELLLIM>(g, rec, gout, c);
+            return;
+        }
+    }
     constexpr int NVAR = DIM + 2;
     const FaceRec<R, DIM> *frec = reinterpret_cast<const FaceRec<R, DIM> *>(g.frec);
     // uniform meshes (all tets, all hexes): the CSR range follows from c, one

@@ -253,14 +253,18 @@ def test_deterministic(tmp_path):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("flux,limiter,mesh", [(1, 3, "j"), (2, 3, "j"), (3, 3, "j"), (3, 5, "j"), (3, 4, "t")],
-                         ids=["ausm", "hll", "hllc", "hllc_venkat", "tets_hllc_bj"])
+@pytest.mark.parametrize("flux,limiter,mesh", [(1, 3, "j"), (2, 3, "j"), (3, 3, "j"), (3, 5, "j"), (3, 4, "t"),
+                                                (3, 5, "t"), (3, 5, "h")],
+                         ids=["ausm", "hll", "hllc", "hllc_venkat", "tets_hllc_bj", "tets_hllc_venkat",
+                              "hexes_hllc_venkat"])
 def test_fp32_close_to_fp64_oracle(tmp_path, flux, limiter, mesh):
     """FP32 state/fluxes with FP64 geometry, RK state and norms: after 30
     iterations the primitive fields stay within 2e-4 relative of the FP64
     oracle (transient, before convergence; the converged error is reported by
     the convergence study). Cell limiters cover the FP32 MUSCL path (limited
-    gradient records, fast divisions in the limiter)."""
+    gradient records, fast divisions in the limiter); quads and tets (4 faces
+    per cell) take the table-driven Green-Gauss gradient, hexes the general
+    one."""
     m = MESH[mesh]()
     path, d, name = make_case(tmp_path, m, max_iter=30, flux=flux, order=2, limiter=limiter, lc=1,
                               mach=3.0 if m.dim == 3 else 2.5)
