@@ -361,6 +361,21 @@ psst_status psst_solver_set_active(psst_solver *s, const int32_t *active);
 psst_status psst_solver_set_stop_rule(psst_solver *s, double drop, int32_t scale_iters, const double *scales,
                                       const int32_t *caps);
 
+/* Merged grids with a stop rule set; no counterpart in the reference. Runs
+ * iterations until every case has stopped, a kernel has raised an error, or
+ * max_iter iterations have run -- as ONE launch of a CUDA graph whose
+ * while-loop node repeats a captured block of `chunk` iterations; the block's
+ * last kernel sets the loop condition on the device from the cases' run
+ * flags, the error word and the iteration count, so the host takes no part
+ * until the end (at most ceil(max_iter / chunk) blocks run). chunk times the
+ * RK stage count must be even. *iterations receives the iterations run
+ * (whole blocks); res_linf / res_l2 (may be NULL) receive the residual
+ * columns of the first min(*iterations, max_iter) of them, [n][dim+2] as
+ * psst_explicit_solve returns them. Per-case residuals are not kept
+ * (psst_solver_case_status gives each case's stopping iteration). */
+psst_status psst_solver_run_to_stop(psst_solver *s, int64_t max_iter, int chunk, int64_t *iterations,
+                                    double *res_linf, double *res_l2);
+
 /* Merged grids only. Per case (each argument may be NULL): run flag, iterations
  * run under the stop rule, iteration at which the drop was reached (0: not
  * reached), and the normalisation in use [ncase][dim+2]. */

@@ -30,7 +30,7 @@ EXPORTED = [
     "psst_solver_use_graphs", "psst_solver_set_active", "psst_solver_case_residuals",
     "psst_solver_use_wavefront", "psst_solver_set_wait_limit", "psst_solver_schedule_info",
     "psst_solver_set_stop_rule", "psst_solver_case_status", "psst_solver_save_checkpoint",
-    "psst_solver_load_checkpoint",
+    "psst_solver_load_checkpoint", "psst_solver_run_to_stop",
     "psst_mlp_create", "psst_mlp_param_count", "psst_mlp_get_params", "psst_mlp_set_params", "psst_mlp_forward",
     "psst_mlp_gradients", "psst_mlp_train_step", "psst_mlp_set_stream", "psst_mlp_destroy", "psst_tc_gemm_bf16",
     "psst_tc_gemm_bf16_wait", "psst_tc_gemm_bf16_time",
@@ -130,6 +130,7 @@ def load():
         "psst_solver_schedule_info": (I, [P, P]),
         "psst_solver_set_stop_rule": (I, [P, D, ctypes.c_int32, P, P]),
         "psst_solver_case_status": (I, [P, P, P, P, P]),
+        "psst_solver_run_to_stop": (I, [P, I64, I, P, P, P]),
         "psst_solver_save_checkpoint": (I, [P, S]),
         "psst_solver_load_checkpoint": (I, [P, S]),
         "psst_mlp_create": (I, [I, ctypes.c_uint64, ctypes.POINTER(P)]),

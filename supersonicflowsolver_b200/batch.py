@@ -1,14 +1,16 @@
 """Many ramp cases of uneven size and inflow solved together on one GPU.
 
 The cases' grids are merged into one (psst_grid_merge), so every kernel
-launch advances all of them; each iteration chunk is one CUDA-graph replay
-(psst_solver_use_graphs); launch shapes come from the solver's own tuner
+launch advances all of them; launch shapes come from the solver's own tuner
 (psst_solver_autotune). The stop rule runs on the device after every
 iteration (psst_solver_set_stop_rule): each case's residual column,
 normalised by its first five iterations, is checked against the drop, and a
 converged (or capped) case is skipped by every later launch, so it stops at
-exactly its converging iteration whatever the chunk length; the host only
-reads the run flags between chunks to see when all cases have stopped.
+exactly its converging iteration. The whole solve is one CUDA-graph launch
+(psst_solver_run_to_stop): a while-loop node repeats a captured block of
+`chunk` iterations, and the block's last kernel ends the loop on the device
+once no case runs; the host waits once, at the end. (chunked=True instead
+replays one graph per chunk and reads the run flags between chunks.)
 
 Workload (seeded): mesh sizes uniform over {60x20, 120x40, 180x60, 240x80}
 quads (x by y), ramp angle U[5, 20] deg, Mach U[1.8, 4.0], p = 101325 Pa,
@@ -58,14 +60,17 @@ def build_cases(cases, directory, precision=32, flux=3, limiter=5, cfl=0.5, rk_l
     return grids, scheme
 
 
-def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, caps=None):
+def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, caps=None, chunked=False):
     """Iterates all cases until every case has stopped: at the residual drop,
     after caps[i] iterations (optional), or after max_iter. cells[i] =
     interior cells of case i; scales[i] (optional) a fixed residual
     normalisation per case. The stop rule is evaluated on the device after
-    every iteration, so the counts are exact. Returns per case the iteration
-    of the drop (None: not reached) and the iterations run, the
-    normalisations used, timings and the cell-iterations of running cases."""
+    every iteration, so the counts are exact. One CUDA-graph launch for the
+    whole solve (blocks of `chunk` iterations; chunk x RK stages even), or,
+    with chunked=True, one graph replay per chunk with the run flags read in
+    between. Returns per case the iteration of the drop (None: not reached)
+    and the iterations run, the normalisations used, timings and the
+    cell-iterations of running cases."""
     ncase = len(cells)
     cap = np.full(ncase, max_iter, dtype=np.int64)
     if caps is not None:
@@ -73,7 +78,11 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, 
     solver.set_stop_rule(drop, scale_iters=5, scales=scales, caps=np.maximum(cap, 0))
     done, dev_s = 0, 0.0
     t0 = time.perf_counter()
-    while done < max_iter and solver.case_status()["active"].any():
+    if not chunked:
+        if solver.case_status()["active"].any():
+            done = solver.run_to_stop(max_iter, chunk)[0]
+            dev_s = solver.last_stats()[1] / 1000.0
+    while chunked and done < max_iter and solver.case_status()["active"].any():
         n = min(chunk, max_iter - done)
         solver.explicit_solve(n)
         dev_s += solver.last_stats()[1] / 1000.0
@@ -87,7 +96,7 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, 
             "cell_iterations": int(np.dot(ran, np.asarray(cells, dtype=np.int64)))}
 
 
-def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chunk=100):
+def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chunk=100, chunked=False):
     """FP32 until each case's residual has dropped by `switch` (above the FP32
     floor, where FP32 still makes progress), then FP64 from the FP32 state
     down to `drop`. Both phases judge the same absolute residual: the FP32
@@ -106,7 +115,7 @@ def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chu
     s32.use_graphs(True)
     s64.launch_shape(shapes["gradient"], shapes["face"], shapes["cell"])
     s64.use_graphs(True)
-    a = run_batch(s32, cells, drop=switch, max_iter=max_iter, chunk=chunk)
+    a = run_batch(s32, cells, drop=switch, max_iter=max_iter, chunk=chunk, chunked=chunked)
     t0 = time.perf_counter()
     s64.set_state(s32.get_state())
     hand = time.perf_counter() - t0
@@ -114,7 +123,8 @@ def run_mixed(merged, scheme, cells, drop=1e-6, switch=1e-4, max_iter=50000, chu
     # every case keeps the iteration budget of a pure run: max_iter in all
     # (a case that did not reach the switch drop ran max_iter in FP32: cap 0)
     caps = [max_iter - r if x is not None else 0 for x, r in zip(a["iterations"], a["ran"])]
-    b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"], caps=caps)
+    b = run_batch(s64, cells, drop=drop, max_iter=max_iter, chunk=chunk, scales=a["scales"], caps=caps,
+                  chunked=chunked)
     state = s64.get_state()
     s64.close()
     wall = a["wall_s"] + hand + b["wall_s"]
@@ -155,7 +165,9 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--drop", type=float, default=1e-6)
     ap.add_argument("--max-iter", type=int, default=50000)
-    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--chunk", type=int, default=100, help="iterations per captured block")
+    ap.add_argument("--chunked", action="store_true",
+                    help="one graph replay per chunk, run flags read in between (default: one launch)")
     ap.add_argument("--flux", type=int, default=3, help="1 AUSM, 2 HLL, 3 HLLC")
     ap.add_argument("--limiter", type=int, default=5)
     ap.add_argument("--precision", type=int, default=32)
@@ -170,7 +182,7 @@ def main():
             merged = Grid.merge(grids)
             setup_s = time.perf_counter() - t0
             r = run_mixed(merged, sc, [g.ninterior for g in grids], drop=a.drop, switch=a.mixed,
-                          max_iter=a.max_iter, chunk=a.chunk)
+                          max_iter=a.max_iter, chunk=a.chunk, chunked=a.chunked)
         its = [x for x in r["iterations"] if x is not None]
         f32 = [x for x in r["fp32_iterations"] if x is not None]
         f64 = [x for x in r["fp64_iterations"] if x is not None]
@@ -195,7 +207,8 @@ def main():
         setup_s = time.perf_counter() - t0
         shapes = solver.autotune(2)
         solver.use_graphs(True)
-        r = run_batch(solver, [g.ninterior for g in grids], drop=a.drop, max_iter=a.max_iter, chunk=a.chunk)
+        r = run_batch(solver, [g.ninterior for g in grids], drop=a.drop, max_iter=a.max_iter, chunk=a.chunk,
+                      chunked=a.chunked)
     its = [x for x in r["iterations"] if x is not None]
     out = {"cases": a.cases, "seed": a.seed, "flux": a.flux, "limiter": a.limiter, "precision": a.precision,
            "cells": int(merged.ninterior), "setup_s": setup_s,

@@ -146,6 +146,17 @@ struct CaseStop {
     double *scale;        // [ncase][dim+2]
 };
 
+// Device-side state of a run-to-stop launch (psst_solver_run_to_stop): a CUDA
+// graph whose while-loop node repeats a captured block of iterations; the
+// block's last kernel appends its residual columns to the history, counts
+// the iterations and sets the loop condition.
+struct LoopCtl {
+    int64_t done;                 // iterations run by this launch so far
+    int64_t max_iter;             // no further block once done >= max_iter
+    int64_t cap_rows;             // rows of the history
+    double *hist_linf, *hist_l2;  // [cap_rows][dim+2]
+};
+
 // Wavefront schedule of the sequential LocalAccTime1 (the reference's in-loop
 // order, psstFiniteVolumeGrid.cpp:317-323) over many RK stages in one
 // persistent launch. Cell c's level exceeds the level of every interior

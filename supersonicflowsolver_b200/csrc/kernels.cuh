@@ -1116,6 +1116,33 @@ __global__ void __launch_bounds__(256) k_case_stop(CaseStop cs, const unsigned l
     if (cs.active[c] && rows >= cs.cap[c]) cs.active[c] = 0;
 }
 
+// Last kernel of a run-to-stop block of `chunk` iterations (one block):
+// appends the block's residual columns to the history, counts the
+// iterations, and sets the while-loop condition: another block while a case
+// still runs, no kernel has raised an error and fewer than max_iter
+// iterations have run. The loop therefore ends after at most
+// ceil(max_iter / chunk) blocks whatever the cases do.
+template <int NV>
+__global__ void __launch_bounds__(256) k_loop_control(CaseStop cs, int32_t ncase, const int32_t *err, LoopCtl *ctl,
+                                                      const double *linf, const double *l2, int32_t chunk,
+                                                      cudaGraphConditionalHandle h) {
+    int any = 0;
+    for (int32_t c = threadIdx.x; c < ncase; c += blockDim.x) any |= cs.active[c] != 0;
+    any = __syncthreads_or(any);
+    const int64_t done = ctl->done, cap = ctl->cap_rows;
+    for (int64_t i = threadIdx.x; i < (int64_t)chunk * NV; i += blockDim.x) {
+        if (done + i / NV >= cap) break;
+        ctl->hist_linf[done * NV + i] = linf[i];
+        ctl->hist_l2[done * NV + i] = l2[i];
+    }
+    __syncthreads();  // every thread has read ctl->done
+    if (threadIdx.x == 0) {
+        const int64_t now = done + chunk;
+        ctl->done = now;
+        cudaGraphSetConditional(h, any && err[0] == 0 && now < ctl->max_iter ? 1u : 0u);
+    }
+}
+
 // Block partials of the residual norms without a block barrier: each warp
 // reduces its lanes (shuffle trees) into a shared slot, and the last warp of
 // the block to arrive sums the slots in warp order and writes out[2 NV] (sum

@@ -65,6 +65,10 @@ struct Ops {
     // merged grids: the per-case stop rule after iteration it_slot
     static void case_stop(int dim, const DevGrid &g, const DevWork<R> &wk, const CaseStop &cs, int it_slot,
                           cudaStream_t s);
+    // the last kernel of a run-to-stop block of `chunk` iterations: history,
+    // iteration count and the while-loop condition `h`
+    static void loop_control(int dim, const DevGrid &g, const DevWork<R> &wk, const CaseStop &cs, LoopCtl *ctl,
+                             int chunk, cudaGraphConditionalHandle h, cudaStream_t s);
     // Sequential LocalAccTime1 over a whole call as one cooperative launch of
     // nblocks CTAs (k_wavefront; FP64 only, cudaErrorNotSupported otherwise).
     static cudaError_t wavefront(int dim, int rec, int lim, const WfArgs<R> &a, int nblocks, cudaStream_t s);

@@ -269,6 +269,15 @@ void Ops<R>::case_stop(int dim, const DevGrid &g, const DevWork<R> &wk, const Ca
         k_case_stop<5><<<nblocks(g.ncase), kBlock, 0, s>>>(cs, cl, g.ncase);
 }
 
+template <typename R>
+void Ops<R>::loop_control(int dim, const DevGrid &g, const DevWork<R> &wk, const CaseStop &cs, LoopCtl *ctl,
+                          int chunk, cudaGraphConditionalHandle h, cudaStream_t s) {
+    if (dim == 2)
+        k_loop_control<4><<<1, kBlock, 0, s>>>(cs, g.ncase, wk.err, ctl, wk.linf, wk.l2, chunk, h);
+    else
+        k_loop_control<5><<<1, kBlock, 0, s>>>(cs, g.ncase, wk.err, ctl, wk.linf, wk.l2, chunk, h);
+}
+
 // ---- sequential LocalAccTime1 as one persistent launch (FP64 only) ----
 template <typename R, int DIM>
 static cudaError_t wavefront_d(int rec, int lim, const WfArgs<R> &a, int nb, cudaStream_t s) {

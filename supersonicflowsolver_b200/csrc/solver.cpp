@@ -475,16 +475,21 @@ struct psst_solver {
     // stream synchronisation per call, no pageable-memory copies
     double *hnorm = nullptr;
     size_t hnorm_cap = 0;
-    // CUDA graphs of whole psst_explicit_solve calls, keyed by (n_iter, buffer parity)
+    // CUDA graphs of whole psst_explicit_solve calls, keyed by (n_iter, buffer
+    // parity), and of run-to-stop launches, keyed by (-chunk, buffer parity)
     bool use_graphs = false;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     std::map<std::pair<int, int>, int64_t> graph_launches;
-    // sequential LocalAccTime1 as one persistent launch per call (FP64, single
-    // grids): schedule uploaded (wf_ready), switched on (wf_on), CTAs, and the
-    // bound of every grid-barrier wait
     // merged grids: the per-case stop rule evaluated on the device (CaseStop)
     bool stop_on = false;
     CaseStop stop{};
+    // run-to-stop launches: the loop's control block and residual history
+    LoopCtl *loopctl = nullptr;
+    double *hist_linf = nullptr, *hist_l2 = nullptr;
+    int64_t hist_rows = 0;
+    // sequential LocalAccTime1 as one persistent launch per call (FP64, single
+    // grids): schedule uploaded (wf_ready), switched on (wf_on), CTAs, and the
+    // bound of every grid-barrier wait
     bool wf_ready = false, wf_on = true;
     WfSched wf{};
     int wf_blocks = 0;
@@ -819,6 +824,95 @@ void run(psst_solver *s, int n_iter, double *res_linf, double *res_l2) {
     s->iter += n_iter;
     if (res_linf) std::memcpy(res_linf, li, nn * sizeof(double));
     if (res_l2) std::memcpy(res_l2, l2, nn * sizeof(double));
+}
+
+// Iterations under the case stop rule until every case has stopped, an error
+// is raised or max_iter iterations have run, as ONE launch of a CUDA graph: a
+// while-loop node repeats a captured block of `chunk` iterations whose last
+// kernel (k_loop_control) sets the loop's condition on the device. The host
+// waits once, at the end. chunk * RK stages must be even, so every block
+// starts on the same state buffer (one captured body serves every pass).
+// Returns the iterations run (whole blocks); the residual columns of the
+// first min(that, max_iter) iterations go to res_linf / res_l2.
+template <typename R>
+int64_t run_to_stop(psst_solver *s, int64_t max_iter, int chunk, double *res_linf, double *res_l2) {
+    DevWork<R> &w = work<R>(s);
+    if (!s->stop_on) raise(PSST_ERR_STATE, "psst_solver_run_to_stop: no stop rule set (psst_solver_set_stop_rule)");
+    if (wavefront_active(s)) raise(PSST_ERR_UNSUPPORTED, "psst_solver_run_to_stop: not with the sequential mode");
+    if ((int64_t)chunk * s->sc.rk_level % 2)
+        raise(PSST_ERR_ARG, "psst_solver_run_to_stop: chunk * RK stages must be even");
+    reserve_norms<R>(s, chunk);
+    const int64_t rows = (max_iter + chunk - 1) / chunk * chunk;
+    if (!s->loopctl) s->loopctl = s->dalloc<LoopCtl>(1);
+    if (rows > s->hist_rows) {  // the graph reads the history's address from the control block
+        ck(cudaStreamSynchronize(s->stream), "stream sync");
+        s->dfree(s->hist_linf);
+        s->dfree(s->hist_l2);
+        s->hist_linf = s->dalloc<double>((size_t)rows * s->nv);
+        s->hist_l2 = s->dalloc<double>((size_t)rows * s->nv);
+        s->hist_rows = rows;
+    }
+    const LoopCtl ctl{0, max_iter, s->hist_rows, s->hist_linf, s->hist_l2};
+    ck(cudaMemcpyAsync(s->loopctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, s->stream), "loop control");
+    const std::pair<int, int> key(-chunk, s->cur);
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+        cudaGraph_t gr = nullptr;
+        ck(cudaGraphCreate(&gr, 0), "graph");
+        int64_t launches = 0;
+        try {
+            cudaGraphConditionalHandle h;
+            ck(cudaGraphConditionalHandleCreate(&h, gr, 1, cudaGraphCondAssignDefault), "graph condition");
+            cudaGraphNodeParams p{};
+            p.type = cudaGraphNodeTypeConditional;
+            p.conditional.handle = h;
+            p.conditional.type = cudaGraphCondTypeWhile;
+            p.conditional.size = 1;
+            cudaGraphNode_t node;
+            ck(cudaGraphAddNode(&node, gr, nullptr, 0, &p), "graph loop node");
+            cudaGraph_t body = p.conditional.phGraph_out[0];
+            ck(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "graph capture");
+            try {
+                zero_norms<R>(s, chunk);
+                iterations<R>(s, chunk, [&](int) { ++launches; });
+                Ops<R>::loop_control(s->dim, s->g, w, s->stop, s->loopctl, chunk, h, s->stream);
+                ++launches;
+            } catch (...) {
+                cudaGraph_t dummy = nullptr;
+                cudaStreamEndCapture(s->stream, &dummy);
+                throw;
+            }
+            ck(cudaStreamEndCapture(s->stream, &body), "graph capture");
+            cudaGraphExec_t ex = nullptr;
+            ck(cudaGraphInstantiate(&ex, gr, 0), "graph instantiate");
+            it = s->graphs.emplace(key, ex).first;
+            s->graph_launches[key] = launches;
+        } catch (...) {
+            cudaGraphDestroy(gr);
+            throw;
+        }
+        cudaGraphDestroy(gr);
+    }
+    ck(cudaEventRecord(s->ev0, s->stream), "event");
+    ck(cudaGraphLaunch(it->second, s->stream), "graph launch");
+    ck(cudaEventRecord(s->ev1, s->stream), "event");
+    LoopCtl out{};
+    int32_t e[4] = {0, 0, 0, 0};
+    ck(cudaMemcpyAsync(&out, s->loopctl, sizeof out, cudaMemcpyDeviceToHost, s->stream), "loop control");
+    ck(cudaMemcpyAsync(e, w.err, sizeof e, cudaMemcpyDeviceToHost, s->stream), "err copy");
+    ck(cudaStreamSynchronize(s->stream), "stream sync");
+    raise_err(s, e, w.err);
+    const size_t n = (size_t)std::min(out.done, max_iter) * s->nv;
+    if (res_linf) ck(cudaMemcpy(res_linf, s->hist_linf, n * sizeof(double), cudaMemcpyDeviceToHost), "history");
+    if (res_l2) ck(cudaMemcpy(res_l2, s->hist_l2, n * sizeof(double), cudaMemcpyDeviceToHost), "history");
+    float ms = 0.0f;
+    ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
+    s->last_ms = ms;
+    s->last_launches = s->graph_launches[key] * (out.done / chunk);
+    s->last_n = 0;  // the per-case residual buffers hold only the last block
+    s->iter += out.done;
+    return out.done;
 }
 
 template <typename R>
@@ -1348,6 +1442,17 @@ extern "C" psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *r
     if (n_iter == 0) return PSST_OK;
     ck(cudaSetDevice(s->device), "cudaSetDevice");
     DISPATCH(s, run)(s, n_iter, res_linf, res_l2);
+    PSST_API_END
+}
+
+extern "C" psst_status psst_solver_run_to_stop(psst_solver *s, int64_t max_iter, int chunk, int64_t *iterations,
+                                               double *res_linf, double *res_l2) {
+    PSST_API_BEGIN
+    if (!s || !iterations) raise(PSST_ERR_ARG, "psst_solver_run_to_stop: null argument");
+    if (!s->has_state) raise(PSST_ERR_STATE, "no state set");
+    if (max_iter < 1 || chunk < 1) raise(PSST_ERR_ARG, "psst_solver_run_to_stop: max_iter and chunk must be >= 1");
+    ck(cudaSetDevice(s->device), "cudaSetDevice");
+    *iterations = DISPATCH(s, run_to_stop)(s, max_iter, chunk, res_linf, res_l2);
     PSST_API_END
 }
 

@@ -305,6 +305,19 @@ class Solver:
         check(_lib.load().psst_solver_set_stop_rule(self._h, float(drop), int(scale_iters),
                                                     None if sc is None else _ptr(sc), None if cp is None else _ptr(cp)))
 
+    def run_to_stop(self, max_iter, chunk=100):
+        """Merged grids with a stop rule: iterates until every case has stopped
+        (or max_iter iterations) as one CUDA-graph launch whose while-loop node
+        the device ends; see psst_solver_run_to_stop. Returns (iterations run,
+        linf, l2), the residual columns [n][dim+2] of those iterations."""
+        n = ctypes.c_int64()
+        li = np.zeros((int(max_iter), self.nv))
+        l2 = np.zeros((int(max_iter), self.nv))
+        check(_lib.load().psst_solver_run_to_stop(self._h, int(max_iter), int(chunk), ctypes.byref(n), _ptr(li),
+                                                  _ptr(l2)))
+        k = min(n.value, int(max_iter))
+        return n.value, li[:k], l2[:k]
+
     def case_status(self):
         """Merged grids: {"active", "iterations", "converged_at", "scales"} per case."""
         ncase = len(self.grid.cases()) - 1

@@ -208,6 +208,48 @@ def test_device_stop_rule_stops_each_case_at_its_own_iteration(tmp_path):
         assert np.array_equal(case_part(state, m, i, 4), solo_state[i]), "case %d" % i
 
 
+@pytest.mark.gpu
+def test_run_to_stop_is_one_launch_with_the_same_result(tmp_path):
+    """psst_solver_run_to_stop: one CUDA-graph launch whose while-loop node the
+    device ends once no case runs. Each case stops at the same iteration, the
+    final state and the merged residual columns equal those of host-driven
+    chunked calls bit for bit; the loop runs whole blocks and no more blocks
+    than max_iter allows; an odd chunk x RK-stage count is refused."""
+    cases = [(12, 4, 10.0, 2.5), (16, 6, 15.0, 3.0), (10, 4, 8.0, 2.2)]
+    grids, schemes, prims, m = build(tmp_path, cases=cases, flux=2, order=1, cfl=0.8, rk_level=1)
+    drop, caps = 0.05, [3000, 3000, 7]
+    a = Solver(m, schemes[0])
+    a.set_state(m.initial_state())
+    a.use_graphs(True)
+    a.set_stop_rule(drop, scale_iters=5, caps=caps)
+    rows = []
+    while a.case_status()["active"].any():
+        rows.append(a.explicit_solve(13)[0])
+    ref_linf = np.concatenate(rows)
+    b = Solver(m, schemes[0])
+    b.set_state(m.initial_state())
+    b.set_stop_rule(drop, scale_iters=5, caps=caps)
+    n, linf, l2 = b.run_to_stop(3000, chunk=14)
+    sa, sb = a.case_status(), b.case_status()
+    for k in ("active", "iterations", "converged_at"):
+        assert np.array_equal(sa[k], sb[k]), k
+    assert n % 14 == 0 and n >= int(sb["iterations"].max()) and n - 14 < int(sb["iterations"].max())
+    assert b.last_stats()[0] > 0  # launches counted: the blocks run times the kernels of one block
+    k = min(len(ref_linf), len(linf))
+    assert np.array_equal(linf[:k], ref_linf[:k])
+    assert np.array_equal(a.get_state(), b.get_state())
+    # the iteration bound ends the loop with cases still running
+    c = Solver(m, schemes[0])
+    c.set_state(m.initial_state())
+    c.set_stop_rule(drop, scale_iters=5)
+    n, linf, _ = c.run_to_stop(20, chunk=14)
+    st = c.case_status()
+    assert n == 28 and len(linf) == 20 and st["active"].any()
+    assert all(it == 28 for it, on in zip(st["iterations"], st["active"]) if on)
+    with pytest.raises(PsstError):
+        c.run_to_stop(20, chunk=7)
+
+
 def test_unconverged_summary_bins_every_case():
     from supersonicflowsolver_b200 import batch as bt
 
