@@ -257,7 +257,9 @@ psst_status psst_explicit_solve(psst_solver *s, int n_iter, double *res_linf, do
 psst_status psst_solver_get_array(psst_solver *s, const char *name, double *out, int64_t count);
 
 /* Runs the solver's work on the given CUDA stream (cudaStream_t passed as a
- * pointer) instead of its own; NULL restores its own stream. */
+ * pointer) instead of its own; NULL restores its own (non-blocking) stream,
+ * so the legacy default stream is selected by its explicit handle,
+ * cudaStreamLegacy. */
 psst_status psst_solver_set_stream(psst_solver *s, void *stream);
 
 /* Kernel launches issued by the last psst_explicit_solve call, and the
@@ -439,9 +441,11 @@ psst_status psst_mlp_gradients(psst_mlp *m, const float *x, const float *t, int 
  * before the step. */
 psst_status psst_mlp_train_step(psst_mlp *m, const float *x, const float *t, int B, float lr, float *loss);
 /* The network's kernels run on `stream` (a cudaStream_t; NULL: its own
- * non-blocking stream). x, t and y are device arrays read and written in
- * stream order: inputs produced on another stream must be complete before a
- * call, and y of psst_mlp_forward is complete only in `stream`'s order. */
+ * non-blocking stream, which is not ordered with the legacy default stream --
+ * select that one by its explicit handle, cudaStreamLegacy). x, t and y are
+ * device arrays read and written in stream order: inputs produced on another
+ * stream must be complete before a call, and y of psst_mlp_forward is
+ * complete only in `stream`'s order. */
 psst_status psst_mlp_set_stream(psst_mlp *m, void *stream);
 void psst_mlp_destroy(psst_mlp *m);
 

@@ -1189,66 +1189,66 @@ __device__ __forceinline__ void lastwarp_partials(double sq[NV], double mx[NV], 
 // its nstage stages (part[stage][nblk][2 NV]): per stage the RMS over the
 // interior cells and the max |res|, then the max over stages (the reference's
 // column is max over stages and cells, psstFiniteVolumeGrid.cpp:331-332; the
-// RMS column is this project's). Block g reduces a fixed range of partials of
-// every stage into mid[g][stage]; the last block to finish combines them in
-// block order (reproducible for a given nblk and grid).
+// RMS column is this project's). Block (g, stage) takes a fixed range of that
+// stage's partials; with 64 NV threads, thread t always reads component
+// t % (2 NV) (consecutive threads read consecutive doubles), and the 32
+// threads of a component are folded in thread order into mid[g][stage][2 NV].
+// The last block to finish folds, per (stage, component), eight fixed
+// sub-ranges of the blocks in parallel and then the eight in order
+// (reproducible for a given nblk and grid).
 template <int NV>
-__global__ void __launch_bounds__(256) k_norm_reduce(const double *part, int nblk, int nstage, int32_t nint,
-                                                     double *mid, unsigned *ticket, double *linf, double *l2,
-                                                     int it_slot) {
-    __shared__ double red[2 * NV][8];
+__global__ void __launch_bounds__(64 * NV) k_norm_reduce(const double *part, int nblk, int nstage, int32_t nint,
+                                                         double *mid, unsigned *ticket, double *linf, double *l2,
+                                                         int it_slot) {
+    constexpr int W = 2 * NV, T = 32 * W, kSplit = 8, kMaxStage = 16;
+    __shared__ double red[T];
+    __shared__ double fin8[kMaxStage * W * kSplit];
     __shared__ bool is_last;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    const int chunk = (nblk + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int t = threadIdx.x, comp = t % W, st = (int)blockIdx.y, G = (int)gridDim.x;
+    const int chunk = (nblk + G - 1) / G;
     const int b0 = (int)blockIdx.x * chunk, b1 = min(nblk, b0 + chunk);
-    for (int st = 0; st < nstage; ++st) {
-        double s[NV], m[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) s[v] = m[v] = 0.0;
-        const double *p = part + (int64_t)st * nblk * 2 * NV;
-        for (int b = b0 + t; b < b1; b += blockDim.x)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                s[v] += p[(int64_t)b * 2 * NV + v];
-                m[v] = fmax(m[v], p[(int64_t)b * 2 * NV + NV + v]);
-            }
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                s[v] += __shfl_down_sync(FULL, s[v], o);
-                m[v] = fmax(m[v], __shfl_down_sync(FULL, m[v], o));
-            }
-            if (lane == 0) {
-                red[v][wid] = s[v];
-                red[NV + v][wid] = m[v];
-            }
-        }
-        __syncthreads();
-        if (t < 2 * NV) {
-            double a = 0.0;
-            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) a = t < NV ? a + red[t][i] : fmax(a, red[t][i]);
-            mid[((int64_t)blockIdx.x * nstage + st) * 2 * NV + t] = a;
-        }
-        __syncthreads();
-    }
-    if (t < 2 * NV) __threadfence();
+    const double *p = part + (int64_t)st * nblk * W;
+    double a = 0.0;  // sums of res^2 and maxima of |res| are both >= 0
+#pragma unroll 4
+    for (int64_t e = (int64_t)b0 * W + t; e < (int64_t)b1 * W; e += T) a = comp < NV ? a + p[e] : fmax(a, p[e]);
+    red[t] = a;
     __syncthreads();
-    if (t == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (t < W) {
+        double v = 0.0;
+        for (int j = 0; j < 32; ++j) v = t < NV ? v + red[t + W * j] : fmax(v, red[t + W * j]);
+        mid[((int64_t)blockIdx.x * nstage + st) * W + t] = v;
+        __threadfence();
+    }
+    __syncthreads();
+    if (t == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y - 1;
     __syncthreads();
     if (!is_last) return;
     __threadfence();
+    const int npair = nstage * W, per = (G + kSplit - 1) / kSplit;
+    for (int q = t; q < npair * kSplit; q += T) {
+        const int pair = q / kSplit, j = q % kSplit, c = pair % W;
+        const int g0 = j * per, g1 = min(G, g0 + per);
+        double v = 0.0;
+#pragma unroll 8
+        for (int g = g0; g < g1; ++g) {
+            const double x = mid[(int64_t)g * npair + pair];  // mid[g][stage][comp]
+            v = c < NV ? v + x : fmax(v, x);
+        }
+        fin8[q] = v;
+    }
+    __syncthreads();
+    if (t < npair) {
+        double v = 0.0;
+        for (int j = 0; j < kSplit; ++j) v = t % W < NV ? v + fin8[t * kSplit + j] : fmax(v, fin8[t * kSplit + j]);
+        red[t] = v;  // npair <= 16 W <= T
+    }
+    __syncthreads();
     if (t < NV) {
         double rms = 0.0, mx = 0.0;
-        for (int st = 0; st < nstage; ++st) {
-            double a = 0.0;
-            for (int g = 0; g < (int)gridDim.x; ++g) {
-                const double *q = mid + ((int64_t)g * nstage + st) * 2 * NV;
-                a += q[t];
-                mx = fmax(mx, q[NV + t]);
-            }
-            const double r = sqrt(a / (double)(nint > 0 ? nint : 1));
+        for (int k = 0; k < nstage; ++k) {
+            const double r = sqrt(red[k * W + t] / (double)(nint > 0 ? nint : 1));
             if (r > rms) rms = r;
+            mx = fmax(mx, red[k * W + NV + t]);
         }
         l2[it_slot * NV + t] = rms;
         linf[it_slot * NV + t] = mx;

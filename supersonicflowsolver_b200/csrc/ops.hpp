@@ -14,7 +14,7 @@ constexpr int kMinBlock = 64;  // smallest launch shape the tuner may pick
 constexpr int kWfBlock = 128;  // threads per CTA of k_wavefront
 constexpr int kWfLanes = 4;    // lanes per cell in k_wavefront's RK stages (cells per work item: 32)
 constexpr int kWfSyncWords = 96;  // k_wavefront's grid-barrier words (three 128-byte lines)
-constexpr int kNormReduceBlocks = 64;  // blocks of k_norm_reduce (first level of its two-level sum)
+constexpr int kNormReduceBlocks = 296;  // blocks of k_norm_reduce (first level of its two-level sum): two per SM
 inline int nblocks(int64_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
 template <typename R>

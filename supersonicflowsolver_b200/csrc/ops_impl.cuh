@@ -185,13 +185,14 @@ void Ops<R>::cell(int dim, int lc, const DevGrid &g, const DevState<R> &cur, con
 template <typename R>
 void Ops<R>::norm_reduce(int dim, const DevGrid &g, const DevWork<R> &wk, int nstage, int it_slot, cudaStream_t s) {
     if (g.nint == 0) return;
-    const int nblk = nblocks(g.nint, g.blk_cell), grid = std::min(nblk, kNormReduceBlocks);
+    const int nblk = nblocks(g.nint, g.blk_cell);
+    const dim3 grid((unsigned)std::min(nblk, kNormReduceBlocks), (unsigned)nstage);
     if (dim == 2)
-        k_norm_reduce<4><<<grid, 256, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
-                                              it_slot);
+        k_norm_reduce<4><<<grid, 64 * 4, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
+                                                 it_slot);
     else
-        k_norm_reduce<5><<<grid, 256, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
-                                              it_slot);
+        k_norm_reduce<5><<<grid, 64 * 5, 0, s>>>(wk.l2part, nblk, nstage, g.nint, wk.l2mid, wk.ticket, wk.linf, wk.l2,
+                                                 it_slot);
 }
 
 template <typename R>

@@ -65,10 +65,12 @@ class MLP:
     def _on_torch_stream(self):
         """The network's kernels run on torch's current stream, in order with
         the kernels that made the input tensors and before any that read the
-        outputs (the library's own stream would race with both)."""
+        outputs (the library's own stream would race with both). Torch's
+        default stream is the legacy NULL stream (handle 0), which the library
+        would take for "its own stream": it is passed as cudaStreamLegacy."""
         import torch
 
-        self.set_stream(torch.cuda.current_stream().cuda_stream)
+        self.set_stream(torch.cuda.current_stream().cuda_stream or CUDA_STREAM_LEGACY)
 
     def forward(self, x):
         """x: torch CUDA FP32 [B][4] -> torch CUDA FP32 [B][4]."""
@@ -107,6 +109,9 @@ class MLP:
             self.close()
         except Exception:
             pass
+
+
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream, by its explicit handle
 
 
 def tc_gemm(A, B, k_split=None, a_strides=None, b_strides=None, M=None, N=None, K=None, wait_polls=None, out=None):

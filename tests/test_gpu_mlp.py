@@ -136,3 +136,24 @@ def test_tc_gemm_wait_that_runs_out_is_reported():
     ref = A.float() @ B.float().T
     bound = (A.float().abs() @ B.float().abs().T) * (512 * 2.0 ** -23) + 1e-6
     assert torch.all((D - ref).abs() <= bound)
+
+
+def test_network_runs_in_order_with_torch_default_stream():
+    """With torch on its default stream (the legacy NULL stream, handle 0), the
+    network's kernels are ordered after the kernels that made their input:
+    an input copied in behind a 25 ms spin kernel is the one the forward pass
+    reads."""
+    from supersonicflowsolver_b200.mlp import MLP
+
+    if not hasattr(torch.cuda, "_sleep"):
+        pytest.skip("torch.cuda._sleep not available")
+    assert torch.cuda.current_stream().cuda_stream == 0
+    net = MLP(seed=1)
+    x_real = torch.rand((1024, 4), device="cuda") * 2.0 - 1.0
+    y_ref = net.forward(x_real).cpu()
+    x = torch.zeros_like(x_real)
+    torch.cuda.synchronize()
+    torch.cuda._sleep(50_000_000)  # about 25 ms of clock cycles on torch's current stream
+    x.copy_(x_real)
+    y = net.forward(x).cpu()
+    assert torch.equal(y, y_ref)

@@ -34,6 +34,12 @@ def test_learned_start_is_closer_and_converges_to_the_same_field():
     pred = ws.predict_prim(net, TEST[0], g, free)
     e_free = field_error(free, pstates[0], g)
     e_pred = field_error(pred, pstates[0], g)
+    import hashlib
+
+    digest = lambda a: hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:12]
+    print("train states %s, params %s, prediction %s; start error rms (free -> learned): %s"
+          % (digest(np.concatenate(states)), digest(net.params()), digest(pred),
+             ", ".join("%s %.3g -> %.3g" % (k, e_free[k]["rms_rel"], e_pred[k]["rms_rel"]) for k in e_free)))
     for k in ("rho", "p", "mach"):
         assert e_pred[k]["rms_rel"] < 0.5 * e_free[k]["rms_rel"], (k, e_pred[k], e_free[k])
 
