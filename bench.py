@@ -411,7 +411,9 @@ def fp64_and_precision(args, grid, sc, prim, fp32_solver, stream_ptr, dev, n_pre
     torch.cuda.synchronize()
     s64.explicit_solve(args.steps)
     ms = s64.last_stats()[1]
+    prof = s64.profile(2)
     rec = {"value": grid.ninterior * args.steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
+           "kernel_ms_per_iteration": {k: t / 2 for k, (t, n) in prof.items()},
            "note": "same mesh, scheme and launch shapes on the FP64 path (FP64 state, fluxes and arithmetic; "
                    "-fmad=false), K iterations in one call replayed as a CUDA graph"}
     # precision: both paths n_prec iterations from the freestream start
