@@ -403,7 +403,7 @@ def fp64_and_precision(args, grid, sc, prim, fp32_solver, stream_ptr, dev, n_pre
     s64 = Solver(grid, sc64, device=dev)
     s64.set_stream(stream_ptr)
     s64.set_state(prim)
-    s64.launch_shape(**fp32_solver.launch_shape())
+    shapes = s64.autotune(2) if not args.no_autotune else s64.launch_shape()
     s64.use_graphs(True)
     s64.explicit_solve(args.warmup)
     s64.explicit_solve(args.steps)
@@ -413,9 +413,9 @@ def fp64_and_precision(args, grid, sc, prim, fp32_solver, stream_ptr, dev, n_pre
     ms = s64.last_stats()[1]
     prof = s64.profile(2)
     rec = {"value": grid.ninterior * args.steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
-           "kernel_ms_per_iteration": {k: t / 2 for k, (t, n) in prof.items()},
-           "note": "same mesh, scheme and launch shapes on the FP64 path (FP64 state, fluxes and arithmetic; "
-                   "-fmad=false), K iterations in one call replayed as a CUDA graph"}
+           "kernel_ms_per_iteration": {k: t / 2 for k, (t, n) in prof.items()}, "threads_per_block": shapes,
+           "note": "same mesh and scheme on the FP64 path (FP64 state, fluxes and arithmetic; -fmad=false), its "
+                   "own tuned launch shapes, K iterations in one call replayed as a CUDA graph"}
     # precision: both paths n_prec iterations from the freestream start
     s64.set_state(prim)
     fp32_solver.set_state(prim)

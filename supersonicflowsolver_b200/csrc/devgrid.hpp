@@ -77,12 +77,14 @@ struct DevGrid {
     const uint64_t *wperm;    // [nint] 4-bit slots: k-th face of the cell's own face order
     const double *lsq_r;      // [3 (2D) or 7 (3D)][nint] least-squares coefficients (reference table)
     const double *vk_eps2;    // [nint] Venkatakrishnan epsilon^2 = (K h)^3, h = V^(1/dim)
-    // FP32 Green-Gauss on meshes of 4 faces per cell (tets, quads), else null:
-    // [2 dim + 1][4 nint] per CSR entry of cell c (slots 4c..4c+3): sign * S/V *
-    // n_k (dim values, sign -1 on side 0), the weight of the neighbour's value
-    // in the face value (1 - beta on side 0, beta on side 1), then the face
-    // offsets x_f - x_c of the cell's side (the face record's o0 / o1)
-    const float *gcoef;
+    // Green-Gauss on meshes of 4 faces per cell (tets, quads), else null; per
+    // CSR entry of cell c (slots 4c..4c+3), component-major [comp][4 nint]:
+    //  FP32 [2 dim + 1]: sign * S/V * n_k (dim values, sign -1 on side 0), the
+    //    weight of the neighbour's value in the face value (1 - beta on side 0,
+    //    beta on side 1), the face offsets x_f - x_c of the cell's side;
+    //  FP64 [2 dim + 2]: sign * (S / V), n_k (dim values), beta, the offsets --
+    //    the values the face records hold, so the arithmetic is unchanged
+    const void *gcoef;
     const int32_t *rank;      // [nint] position in the reference's interior update order
     const int32_t *gptr;      // [nint+1] ghosts of each interior cell (ghost index space)
     const int32_t *g_nb;      // [nghost] interior neighbour of each ghost

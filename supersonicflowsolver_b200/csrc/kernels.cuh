@@ -638,12 +638,100 @@ __device__ __forceinline__ void gradient_cell_table(const DevGrid &g, const Cell
     st16(gout + c, out);
 }
 
+// FP64 (parity) form of the same: the table holds sign * (S/V), n, beta and
+// the offsets exactly as the face records and the general path have them,
+// and the operations below are the general path's in its order
+// (psstGradCalculation.cpp:80-177): tv = beta phi0 + (1 - beta) phi1, then
+// ((sign tv) (S/V)) n_k, where sign tv (S/V) = tv (sign S/V) exactly.
+template <int DIM, int CELLLIM>
+__device__ __forceinline__ void gradient_cell_table64(const DevGrid &g, const CellRec<double> *rec,
+                                                      GradRec<double, DIM> *gout, int32_t c) {
+    constexpr int NVAR = DIM + 2;
+    const int4 nb = *reinterpret_cast<const int4 *>(g.csr_nb + 4 * c);
+    const CellRec<double> r4[4] = {ldg(rec + nb.x), ldg(rec + nb.y), ldg(rec + nb.z), ldg(rec + nb.w)};
+    const Prim<double, DIM> own = unpack<double, DIM>(ldg(rec + c));
+    // entry q of component j; read per face (the cell's 32 bytes of a component
+    // share one line, so the later faces' reads hit L1), which keeps few of the
+    // table's values live at once
+    const double *tab = reinterpret_cast<const double *>(g.gcoef) + 4 * (int64_t)c;
+    auto at = [&](int j, int q) { return __ldg(tab + (int64_t)4 * j * g.nint + q); };
+    double gr[NVAR][DIM], mx[NVAR], mn[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) {
+        mx[i] = mn[i] = pvar<double, DIM>(own, i);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) gr[i][k] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const Prim<double, DIM> oth = unpack<double, DIM>(r4[q]);
+        const double gps = at(0, q), beta = at(DIM + 1, q), rbeta = 1.0 - beta;
+        double nrm[DIM];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) nrm[k] = at(1 + k, q);
+        const bool side = gps > 0.0;
+#pragma unroll
+        for (int i = 0; i < NVAR; ++i) {
+            const double a = pvar<double, DIM>(own, i), o = pvar<double, DIM>(oth, i);
+            if (CELLLIM) {
+                if (o > mx[i]) mx[i] = o;
+                if (o < mn[i]) mn[i] = o;
+            }
+            const double phi0 = side ? o : a, phi1 = side ? a : o;
+            const double tv = beta * phi0 + rbeta * phi1;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) gr[i][k] += tv * gps * nrm[k];
+        }
+    }
+    double lim[NVAR];
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i) lim[i] = 1.0;
+    if (CELLLIM) {
+        const double eps2 = CELLLIM == 5 ? g.vk_eps2[c] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double off[DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) off[k] = at(DIM + 2 + k, q);
+#pragma unroll
+            for (int i = 0; i < NVAR; ++i) {
+                const double phic = pvar<double, DIM>(own, i);
+                double dm = 0.0;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) dm += gr[i][k] * off[k];
+                double pf = 1.0;
+                if (dm != 0.0) {
+                    const double dp = dm > 0.0 ? mx[i] - phic : mn[i] - phic;
+                    if (CELLLIM == 4) {
+                        const double y = dp / dm;
+                        pf = y < 1.0 ? y : 1.0;
+                    } else {
+                        const double num = (dp * dp + eps2) + 2.0 * dm * dp;
+                        const double den = dp * dp + 2.0 * dm * dm + dm * dp + eps2;
+                        pf = num / den;
+                    }
+                }
+                if (pf < lim[i]) lim[i] = pf;
+            }
+        }
+    }
+    GradRec<double, DIM> out;
+#pragma unroll
+    for (int i = 0; i < NVAR; ++i)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) out.g[i * DIM + k] = CELLLIM ? gr[i][k] * lim[i] : gr[i][k];
+    st16(gout + c, out);
+}
+
 template <typename R, int DIM, int GRAD, int CELLLIM, bool CG>
 __device__ __forceinline__ void gradient_cell(const DevGrid &g, const CellRec<R> *rec, GradRec<R, DIM> *gout,
                                               int32_t c) {
-    if constexpr (sizeof(R) == 4 && GRAD == 1 && !CG) {
+    if constexpr (GRAD == 1 && !CG) {
         if (g.gcoef) {
-            gradient_cell_table<DIM, CELLLIM>(g, rec, gout, c);
+            if constexpr (sizeof(R) == 4)
+                gradient_cell_table<DIM, CELLLIM>(g, rec, gout, c);
+            else
+                gradient_cell_table64<DIM, CELLLIM>(g, rec, gout, c);
             return;
         }
     }

@@ -414,28 +414,43 @@ std::vector<FaceRec<R, DIM>> build_face_records(const psst_grid &G, const Layout
     return out;
 }
 
-// The FP32 Green-Gauss table of DevGrid::gcoef (meshes with 4 faces per
-// cell): per CSR entry q = 4c + j, component-major so that a cell's 4 values
-// of one component are one 16-byte load. Products and quotients in FP64, each
-// value rounded to FP32 once; the offsets are the face records' o0 / o1.
-std::vector<float> build_gradient_coefficients(const Layout &L, int dim, int rec) {
+// The Green-Gauss table of DevGrid::gcoef (meshes with 4 faces per cell):
+// per CSR entry q = 4c + j, component-major so that a cell's 4 values of one
+// component are one 16-byte (FP32) or 32-byte (FP64) load. FP32: products and
+// quotients in FP64, each value rounded to FP32 once. FP64: the face record's
+// own values (S / V as the general path divides it, n, beta), so the kernel's
+// arithmetic and its order are the general path's. Offsets: the face
+// records' o0 / o1 (side 0 / side 1), rounded to R as there.
+template <typename R>
+std::vector<R> build_gradient_coefficients(const Layout &L, int dim, int rec) {
+    constexpr bool F64 = sizeof(R) == 8;
     const int64_t ne = (int64_t)4 * L.nint;
-    std::vector<float> out((size_t)(2 * dim + 1) * ne);
+    const int ncomp = 2 * dim + (F64 ? 2 : 1), off0 = F64 ? dim + 2 : dim + 1;
+    std::vector<R> out((size_t)ncomp * ne);
     parallel_for(ne, [&](int64_t q0, int64_t q1) {
         for (int64_t q = q0; q < q1; ++q) {
             const int32_t c = (int32_t)(q / 4), ent = L.csr_ent[q], f = ent >> 1, side = ent & 1;
             const int32_t c0 = L.c0[f], c1 = L.c1[f];
             const double sv = (side ? 1.0 : -1.0) * (L.S[f] / L.V[c]);
             for (int k = 0; k < dim; ++k) {
-                out[(size_t)k * ne + q] = (float)(sv * L.n[(size_t)k * L.nface + f]);
+                const double n = L.n[(size_t)k * L.nface + f];
+                if (F64)
+                    out[(size_t)(1 + k) * ne + q] = (R)n;
+                else
+                    out[(size_t)k * ne + q] = (R)(sv * n);
                 const double xf = L.xf[(size_t)k * L.nface + f];
                 const double x0 = L.xc[(size_t)k * L.nall + c0], x1 = L.xc[(size_t)k * L.nall + c1];
-                float off = 0.0f;  // as build_face_records stores o0 (side 0) / o1 (side 1)
-                if (rec == 1 && !side) off = (float)(x0 - x1);
-                if (rec == 2) off = (float)(xf - (side ? x1 : x0));
-                out[(size_t)(dim + 1 + k) * ne + q] = off;
+                R o = (R)0;  // as build_face_records stores o0 (side 0) / o1 (side 1)
+                if (rec == 1 && !side) o = (R)(x0 - x1);
+                if (rec == 2) o = (R)(xf - (side ? x1 : x0));
+                out[(size_t)(off0 + k) * ne + q] = o;
             }
-            out[(size_t)dim * ne + q] = (float)(side ? L.beta[f] : 1.0 - L.beta[f]);
+            if (F64) {
+                out[q] = (R)sv;  // negation is exact: |sv| is the general path's S / V
+                out[(size_t)(dim + 1) * ne + q] = (R)L.beta[f];
+            } else {
+                out[(size_t)dim * ne + q] = (R)(side ? L.beta[f] : 1.0 - L.beta[f]);
+            }
         }
     });
     return out;
@@ -573,8 +588,8 @@ void alloc_state(psst_solver *s, const psst_grid &G) {
         for (size_t q = 0; q < cs.size(); ++q) cs[q] = (R)s->L.S[s->L.csr_ent[q] >> 1];
         s->g.csr_s = s->upload(cs);
     }
-    if (sizeof(R) == 4 && s->g.kuni == 4 && s->sc.order == 2 && s->sc.grad == 1)
-        s->g.gcoef = s->upload(build_gradient_coefficients(s->L, dim, s->rec));
+    if (s->g.kuni == 4 && s->sc.order == 2 && s->sc.grad == 1)
+        s->g.gcoef = s->upload(build_gradient_coefficients<R>(s->L, dim, s->rec));
     DevState<R> *st = states<R>(s);
     for (int b = 0; b < 2; ++b) {
         st[b].rec = s->dalloc<CellRec<R>>(nall);
