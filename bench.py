@@ -390,6 +390,34 @@ def state_fields(solver, grid, sc):
     return {"rho": solver.get("rho"), "p": prim[:nv], "mach": speed / np.sqrt(sc.gamma * sc.rm * T)}
 
 
+def reference_scheme(args, grid, sc, prim, stream_ptr, dev):
+    """The FP32 path on the same mesh with the limiter the reference arm runs
+    (DM reconstruction + VanLeer, the reference's own scheme; it has no cell
+    limiters): device-resident throughput, its own tuned launch shapes, K
+    iterations in one graph replay -- the figure to set beside the reference
+    arm's per-cell rate."""
+    import torch
+    from supersonicflowsolver_b200.psst import Solver
+
+    sc3 = type(sc).from_buffer_copy(sc)
+    sc3.limiter = CPU_LIMITER
+    s3 = Solver(grid, sc3, device=dev)
+    s3.set_stream(stream_ptr)
+    s3.set_state(prim)
+    shapes = s3.autotune(2) if not args.no_autotune else s3.launch_shape()
+    s3.use_graphs(True)
+    s3.explicit_solve(args.warmup)
+    s3.explicit_solve(args.steps)
+    s3.explicit_solve(args.steps)
+    torch.cuda.synchronize()
+    s3.explicit_solve(args.steps)
+    ms = s3.last_stats()[1]
+    s3.close()
+    return {"value": grid.ninterior * args.steps / (ms / 1000.0), "unit": "cell-updates/s",
+            "ms_per_step": ms / args.steps, "threads_per_block": shapes,
+            "scheme": scheme_text(args.workload).replace("MUSCL/Venkatakrishnan(K=5)", "DM/VanLeer")}
+
+
 def fp64_and_precision(args, grid, sc, prim, fp32_solver, stream_ptr, dev, n_prec=500):
     """The same workload on the FP64 path (the reference's precision): its
     device-resident throughput over `steps` iterations, and the FP32
@@ -585,6 +613,7 @@ def run_gpu(args):
     if args.workload == "wedge3d_6M_tets" and not args.no_fp64 and ws == 1:
         extra["fp64"], extra["precision"] = fp64_and_precision(args, grid, sc, prim, solver, stream.cuda_stream, dev)
     if args.workload == "wedge3d_6M_tets" and ws == 1:
+        extra["reference_scheme"] = reference_scheme(args, grid, sc, prim, stream.cuda_stream, dev)
         extra["tensor_gemm"] = gemm_throughput()
     if rank == 0:
         nv = grid.dim + 2

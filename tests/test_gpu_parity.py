@@ -254,9 +254,9 @@ def test_deterministic(tmp_path):
 
 
 @pytest.mark.parametrize("flux,limiter,mesh", [(1, 3, "j"), (2, 3, "j"), (3, 3, "j"), (3, 5, "j"), (3, 4, "t"),
-                                                (3, 5, "t"), (3, 5, "h")],
+                                                (3, 5, "t"), (3, 5, "h"), (3, 3, "t"), (3, 1, "t"), (2, 2, "h")],
                          ids=["ausm", "hll", "hllc", "hllc_venkat", "tets_hllc_bj", "tets_hllc_venkat",
-                              "hexes_hllc_venkat"])
+                              "hexes_hllc_venkat", "tets_hllc_vanleer", "tets_hllc_vanalbada", "hexes_hll_minmod"])
 def test_fp32_close_to_fp64_oracle(tmp_path, flux, limiter, mesh):
     """FP32 state/fluxes with FP64 geometry, RK state and norms: after 30
     iterations the primitive fields stay within 2e-4 relative of the FP64
@@ -264,7 +264,8 @@ def test_fp32_close_to_fp64_oracle(tmp_path, flux, limiter, mesh):
     the convergence study). Cell limiters cover the FP32 MUSCL path (limited
     gradient records, fast divisions in the limiter); quads and tets (4 faces
     per cell) take the table-driven Green-Gauss gradient, hexes the general
-    one."""
+    one; the reference's limiters (DM reconstruction) use one fast division
+    each on this path."""
     m = MESH[mesh]()
     path, d, name = make_case(tmp_path, m, max_iter=30, flux=flux, order=2, limiter=limiter, lc=1,
                               mach=3.0 if m.dim == 3 else 2.5)
