@@ -250,6 +250,33 @@ def test_run_to_stop_is_one_launch_with_the_same_result(tmp_path):
         c.run_to_stop(20, chunk=7)
 
 
+@pytest.mark.gpu
+def test_run_to_stop_fp32_rk4_matches_chunked_calls(tmp_path):
+    """The single launch on the FP32 path with RK4 and MUSCL (the batched
+    workload's scheme): same stopping iterations and final state as 100-
+    iteration chunked calls; without a stop rule the call is refused."""
+    cases = [(12, 4, 10.0, 2.5), (16, 6, 15.0, 3.0)]
+    grids, schemes, prims, m = build(tmp_path, precision=32, cases=cases, flux=3, order=2, limiter=5, rk_level=4)
+    drop = 1e-3
+    a = Solver(m, schemes[0])
+    a.set_state(m.initial_state())
+    a.use_graphs(True)
+    a.set_stop_rule(drop, scale_iters=5, caps=[4000, 4000])
+    while a.case_status()["active"].any():
+        a.explicit_solve(100)
+    b = Solver(m, schemes[0])
+    b.set_state(m.initial_state())
+    with pytest.raises(PsstError):
+        b.run_to_stop(100, chunk=50)
+    b.set_stop_rule(drop, scale_iters=5, caps=[4000, 4000])
+    n, _, _ = b.run_to_stop(4000, chunk=50)
+    sa, sb = a.case_status(), b.case_status()
+    for k in ("iterations", "converged_at"):
+        assert np.array_equal(sa[k], sb[k]), k
+    assert not sb["active"].any() and n % 50 == 0
+    assert np.array_equal(a.get_state(), b.get_state())
+
+
 def test_unconverged_summary_bins_every_case():
     from supersonicflowsolver_b200 import batch as bt
 
