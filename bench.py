@@ -7,8 +7,10 @@ HLLC flux, cell-limited MUSCL with the Venkatakrishnan limiter (K = 5),
 Green-Gauss gradients, RK4 (the reference's standard coefficients),
 LocalAccTime1 evaluated from stage-start values, CFL 0.5; FP32 state and
 fluxes, FP64 geometry / RK state / residual norms; cells on a Hilbert curve.
-One step = one iteration (4 RK stages) over all cells. Synthetic mesh and
-freestream start: no dataset is involved.
+One step = one iteration (4 RK stages) over all cells; by default the
+timed region is the workload's whole 500-iteration run from the freestream
+start (--steps overrides). Synthetic mesh and freestream start: no dataset
+is involved.
 
   value : cell-updates/s with the state resident in HBM (K iterations in one
           psst_explicit_solve call, replayed as one CUDA graph captured
@@ -48,7 +50,7 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # the bandwidth benchmark: 200x100x50 hexes x 6 tets, FP32, MUSCL/Venkatakrishnan
     "wedge3d_6M_tets": dict(dim=3, mesh=(200, 100, 50), mach=3.0, angle=12.0, precision=32, limiter=5,
-                            cpu_mesh=(40, 20, 4), cpu_procs=0),
+                            cpu_mesh=(40, 20, 4), cpu_procs=0, run_steps=500),
     # small case of the same workload for ncu captures
     "wedge3d_750k_tets": dict(dim=3, mesh=(100, 50, 25), mach=3.0, angle=12.0, precision=32, limiter=5,
                               cpu_mesh=(40, 20, 4), cpu_procs=0),
@@ -673,7 +675,8 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: the workload's run length, e.g. the 6M-tet ramp's 500 iterations)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wedge3d_6M_tets", choices=sorted(WORKLOADS))
@@ -686,6 +689,8 @@ def main():
     ap.add_argument("--gemm-only", action="store_true",
                     help="print only the tensor-core GEMM figures (the tensor_gemm object) and exit")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = WORKLOADS[args.workload].get("run_steps", 20)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.gemm_only:
