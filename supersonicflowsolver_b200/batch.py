@@ -80,7 +80,7 @@ def run_batch(solver, cells, drop=1e-6, max_iter=50000, chunk=100, scales=None, 
     t0 = time.perf_counter()
     if not chunked:
         if solver.case_status()["active"].any():
-            done = solver.run_to_stop(max_iter, chunk)[0]
+            done = solver.run_to_stop(max_iter, chunk, history=False)[0]
             dev_s = solver.last_stats()[1] / 1000.0
     while chunked and done < max_iter and solver.case_status()["active"].any():
         n = min(chunk, max_iter - done)

@@ -857,7 +857,9 @@ int64_t run_to_stop(psst_solver *s, int64_t max_iter, int chunk, double *res_lin
     if ((int64_t)chunk * s->sc.rk_level % 2)
         raise(PSST_ERR_ARG, "psst_solver_run_to_stop: chunk * RK stages must be even");
     reserve_norms<R>(s, chunk);
-    const int64_t rows = (max_iter + chunk - 1) / chunk * chunk;
+    // a history only when the caller wants the residual columns (the loop skips
+    // the copy once the count reaches cap_rows)
+    const int64_t rows = (res_linf || res_l2) ? (max_iter + chunk - 1) / chunk * chunk : 0;
     if (!s->loopctl) s->loopctl = s->dalloc<LoopCtl>(1);
     if (rows > s->hist_rows) {  // the graph reads the history's address from the control block
         ck(cudaStreamSynchronize(s->stream), "stream sync");
@@ -867,7 +869,7 @@ int64_t run_to_stop(psst_solver *s, int64_t max_iter, int chunk, double *res_lin
         s->hist_l2 = s->dalloc<double>((size_t)rows * s->nv);
         s->hist_rows = rows;
     }
-    const LoopCtl ctl{0, max_iter, s->hist_rows, s->hist_linf, s->hist_l2};
+    const LoopCtl ctl{0, max_iter, rows, s->hist_linf, s->hist_l2};
     ck(cudaMemcpyAsync(s->loopctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, s->stream), "loop control");
     const std::pair<int, int> key(-chunk, s->cur);
     auto it = s->graphs.find(key);

@@ -305,16 +305,19 @@ class Solver:
         check(_lib.load().psst_solver_set_stop_rule(self._h, float(drop), int(scale_iters),
                                                     None if sc is None else _ptr(sc), None if cp is None else _ptr(cp)))
 
-    def run_to_stop(self, max_iter, chunk=100):
+    def run_to_stop(self, max_iter, chunk=100, history=True):
         """Merged grids with a stop rule: iterates until every case has stopped
         (or max_iter iterations) as one CUDA-graph launch whose while-loop node
         the device ends; see psst_solver_run_to_stop. Returns (iterations run,
-        linf, l2), the residual columns [n][dim+2] of those iterations."""
+        linf, l2), the residual columns [n][dim+2] of those iterations (None
+        without history)."""
         n = ctypes.c_int64()
-        li = np.zeros((int(max_iter), self.nv))
-        l2 = np.zeros((int(max_iter), self.nv))
-        check(_lib.load().psst_solver_run_to_stop(self._h, int(max_iter), int(chunk), ctypes.byref(n), _ptr(li),
-                                                  _ptr(l2)))
+        li = np.zeros((int(max_iter), self.nv)) if history else None
+        l2 = np.zeros((int(max_iter), self.nv)) if history else None
+        check(_lib.load().psst_solver_run_to_stop(self._h, int(max_iter), int(chunk), ctypes.byref(n),
+                                                  _ptr(li) if history else None, _ptr(l2) if history else None))
+        if not history:
+            return n.value, None, None
         k = min(n.value, int(max_iter))
         return n.value, li[:k], l2[:k]
 
