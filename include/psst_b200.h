@@ -454,15 +454,18 @@ void psst_mlp_destroy(psst_mlp *m);
  * (A[m][k] = A[m*a_sm + k*a_sk], B[n][k] = B[n*b_sn + k*b_sk]), FP32 device
  * output with row stride d_sm, z over ceil(K / k_split) splits (plain element
  * sum of the splits = the full product). Synchronises the stream. Operands
- * contiguous along K (a_sk or b_sk == 1) or along M/N (a_sm or b_sn == 1, the
- * other stride a multiple of 8) load as 16-byte vectors; other strides
- * element by element. */
+ * 16-byte aligned with a row stride of a multiple of 8 elements, contiguous
+ * along K (a_sk or b_sk == 1) or along M/N (a_sm or b_sn == 1), with split
+ * ranges of whole 64-wide chunks (k_split % 64 == 0, or one split), are
+ * loaded by TMA (tensor maps encoded per call); other operands are staged
+ * through registers (16-byte vectors where aligned, else element by element). */
 psst_status psst_tc_gemm_bf16(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn, int64_t b_sk,
                               int M, int N, int K, int k_split, float *D, int64_t d_sm, void *stream);
 
-/* psst_tc_gemm_bf16 launched reps times back to back between two CUDA events
- * on `stream`; *ms receives the mean device time of one launch (the GEMM's
- * throughput without the per-call synchronisation). */
+/* psst_tc_gemm_bf16 timed: one launch outside the timing, then reps launches
+ * captured as one CUDA graph on a private stream (ordered after `stream`) and
+ * replayed between two CUDA events; *ms receives the mean device time of one
+ * launch, with no host time between launches. */
 psst_status psst_tc_gemm_bf16_time(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
                                    int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
                                    void *stream, int reps, double *ms);
