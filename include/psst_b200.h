@@ -472,10 +472,11 @@ psst_status psst_tc_gemm_bf16_time(const void *A, int64_t a_sm, int64_t a_sk, co
 
 /* psst_tc_gemm_bf16 with the bound of its first mbarrier wait that runs out
  * given in polls (< 0: the default, about a second; 0: that wait gives up at
- * once). A wait that runs out makes the call return PSST_ERR_TIMEOUT after a
- * second, full-length wait for the tensor-core work in flight, so no MMA is
- * running when the kernel frees its tensor memory; D is then undefined. Used
- * to test the timeout path without stalling a GPU. */
+ * once). A wait that runs out makes the call return PSST_ERR_TIMEOUT after
+ * full-length waits for the tensor-core work and the TMA copies in flight, so
+ * no MMA or copy is running when the kernel frees its tensor memory and its
+ * shared memory; D is then undefined. Used to test the timeout path without
+ * stalling a GPU. */
 psst_status psst_tc_gemm_bf16_wait(const void *A, int64_t a_sm, int64_t a_sk, const void *B, int64_t b_sn,
                                    int64_t b_sk, int M, int N, int K, int k_split, float *D, int64_t d_sm,
                                    void *stream, int64_t wait_polls);
