@@ -493,6 +493,29 @@ def gemm_throughput():
         bound = min(peak, flops / (byts / (hbm * 1e9)) / 1e12)
         out[name] = {"ms": ms, "tflops": tf, "frac_of_peak": tf / peak, "hbm_bound_tflops": bound,
                      "frac_of_shape_bound": tf / bound}
+    del S, T
+    # one whole training step of the warm-start network (forward, backward,
+    # Adam, the loss read back), batch 16384: wall time per step
+    from supersonicflowsolver_b200.mlp import MLP
+
+    net = MLP(seed=0)
+    xb = torch.rand((16384, 4), generator=g, device="cuda") * 2.0 - 1.0
+    tb = torch.rand((16384, 4), generator=g, device="cuda")
+    for _ in range(3):
+        net.train_step(xb, tb, 1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        net.train_step(xb, tb, 1e-3)
+    torch.cuda.synchronize()
+    step_ms = (time.perf_counter() - t0) * 1000.0 / 20
+    # 5 forward, 5 weight-gradient and 4 data-gradient GEMMs (none into the features)
+    gemm_flops = 2.0 * 16384 * (3 * (256 * 128 + 4 * 256 * 256) - 256 * 128)
+    out["mlp_train_step_16384"] = {"ms": step_ms, "gemm_tflops_effective": gemm_flops / (step_ms * 1e-3) / 1e12,
+                                   "note": "wall time per step (it reads the loss back, so each step waits for "
+                                           "its kernels); 14 tensor-core GEMMs plus features, output layer, "
+                                           "reductions and Adam"}
+    net.close()
     return out
 
 
