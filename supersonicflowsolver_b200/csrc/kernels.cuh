@@ -262,6 +262,15 @@ __device__ __forceinline__ R pvar(const Prim<R, DIM> &s, int i) {
     return i < DIM ? s.u[i] : (i == DIM ? s.p : s.T);
 }
 
+// Division of several numerators by one denominator: FP32, one reciprocal
+// and a product each; FP64 (parity), the reference's division each.
+template <typename R>
+struct SharedDen {
+    R d, r;
+    __device__ __forceinline__ explicit SharedDen(R den) : d(den), r(sizeof(R) == 4 ? (R)1 / den : (R)0) {}
+    __device__ __forceinline__ R operator()(R num) const { return sizeof(R) == 4 ? num * r : num / d; }
+};
+
 // psstConvectiveFlow.cpp:13-24
 template <typename R>
 __device__ __forceinline__ R roe_avg(R lv, R rv, R ld, R rd) {
@@ -438,9 +447,9 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
         } else if (s1 <= (R)0 && s0 >= (R)0) {
             side(0, f0, w0);
             side(1, f1, w1);
+            const SharedDen<R> q(s0 - s1);
 #pragma unroll
-            for (int j = 0; j < DIM + 2; ++j)
-                flow[j] = (s0 * f1[j] - s1 * f0[j] + s0 * s1 * (w0[j] - w1[j])) / (s0 - s1);
+            for (int j = 0; j < DIM + 2; ++j) flow[j] = q(s0 * f1[j] - s1 * f0[j] + s0 * s1 * (w0[j] - w1[j]));
         } else if (s0 <= (R)0) {
             side(0, f0, w0);
 #pragma unroll
@@ -468,15 +477,16 @@ __device__ __forceinline__ bool interior_flux(Prim<R, DIM> r[2], const GradRec<R
             side(1, fs, ws);
         else
             side(0, fs, ws);
+        const SharedDen<R> q(tt);
 #pragma unroll
         for (int j = 0; j < DIM + 2; ++j) {
             const R wj = ws[j], fj = fs[j];
             if (j < DIM)
-                flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * nn[j]) / tt;
+                flow[j] = q(sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * nn[j]);
             else if (j == DIM)
-                flow[j] = (sh * (ss * wj - fj)) / tt;
+                flow[j] = q(sh * (ss * wj - fj));
             else
-                flow[j] = (sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * sh) / tt;
+                flow[j] = q(sh * (ss * wj - fj) + ss * (pr + dd * (ss - vv) * (sh - vv)) * sh);
         }
     } else if (s0 <= (R)0) {
         side(0, fs, ws);
